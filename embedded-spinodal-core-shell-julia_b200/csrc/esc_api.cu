@@ -1,0 +1,576 @@
+// C ABI host library: contexts, batches, CUDA-graph step chunks.
+//
+// The public entry points mirror the Julia driver core_shell.jl:84-103
+// (run_simulation).  A context is a batch of one.  A batch groups its
+// instances by grid size; each group owns contiguous device buffers and a
+// device array of instance descriptors, and every phase kernel of a step is one
+// launch per group whose grid is (tiles, instances).  Steps are replayed from a
+// captured CUDA graph of kChunk steps; a device-side step counter gives each
+// launch its history row, so the graph never needs re-instantiation.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "esc.h"
+#include "esc_dispatch.cuh"
+
+#define ESC_DECL(n) const esc::KernelSet* esc_kernels_##n(int prec);
+ESC_SIZES(ESC_DECL)
+#undef ESC_DECL
+
+namespace {
+
+const esc::KernelSet* find_kernels(int n, int prec) {
+  switch (n) {
+#define ESC_CASE(nn) \
+  case nn:           \
+    return esc_kernels_##nn(prec);
+    ESC_SIZES(ESC_CASE)
+#undef ESC_CASE
+    default:
+      return nullptr;
+  }
+}
+
+thread_local std::string tl_err;
+
+// Advances the device-side step counter read by the phase kernels.
+__global__ void k_advance(int* base, int by) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *base += by;
+}
+constexpr int kChunk = 32;  // steps per captured graph
+
+struct Group {
+  const esc::KernelSet* ks = nullptr;
+  int n = 0;
+  std::vector<int> members;  // batch indices, in slot order
+  void* S = nullptr;
+  void* F = nullptr;
+  void* G = nullptr;
+  void* phi = nullptr;
+  void* tw_s = nullptr;
+  void* tw_w = nullptr;
+  double* cio = nullptr;
+  double* part = nullptr;
+  double* scal = nullptr;
+  unsigned* cnt = nullptr;
+  int* status = nullptr;
+  long long* bad = nullptr;
+  esc::InstDev* d_inst = nullptr;
+  std::vector<esc::InstDev> h_inst;
+};
+
+struct Engine {
+  int count = 0;
+  int prec = 0;
+  int device = 0;
+  std::vector<int> n;
+  std::vector<double> dx;
+  std::vector<esc::ModelParams> p;
+  std::vector<Group> groups;
+  std::vector<std::pair<int, int>> where;  // instance -> (group, slot)
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  int* base = nullptr;
+  double* hist = nullptr;
+  size_t hist_cap = 0;  // doubles
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<void*> allocs;
+  std::string err;
+
+  esc_status fail(esc_status s, const std::string& msg) {
+    err = msg;
+    tl_err = msg;
+    return s;
+  }
+  esc_status fail_cuda(const char* what, cudaError_t e) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    return fail(e == cudaErrorMemoryAllocation ? ESC_ENOMEM : ESC_ECUDA, buf);
+  }
+
+  template <typename T>
+  esc_status alloc(T** ptr, size_t bytes, const char* what) {
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+    if (e != cudaSuccess) return fail_cuda(what, e);
+    allocs.push_back(q);
+    *ptr = static_cast<T*>(q);
+    return ESC_OK;
+  }
+
+  void release() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    for (void* q : allocs) cudaFree(q);
+    allocs.clear();
+    if (own) cudaStreamDestroy(own);
+    own = nullptr;
+  }
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define CK(call)                                             \
+  do {                                                       \
+    const cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return E.fail_cuda(#call, e_);    \
+  } while (0)
+#define TRY(call)                         \
+  do {                                    \
+    const esc_status s_ = (call);         \
+    if (s_ != ESC_OK) return s_;          \
+  } while (0)
+
+bool finite_params(const esc_params& q) {
+  const double v[10] = {q.A, q.B, q.chi, q.P, q.ca, q.cb, q.cc, q.kappa, q.mobility, q.Q};
+  for (double x : v)
+    if (!std::isfinite(x)) return false;
+  return true;
+}
+
+// e^{-2 pi i j / n}, j < n, from long-double trigonometry, written as `real` pairs.
+template <typename real>
+std::vector<real> twiddles(int n) {
+  std::vector<real> t(2 * (size_t)n);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int j = 0; j < n; ++j) {
+    const long double a = two_pi * (long double)j / (long double)n;
+    t[2 * (size_t)j] = (real)cosl(a);
+    t[2 * (size_t)j + 1] = (real)(-sinl(a));
+  }
+  return t;
+}
+
+esc_status engine_create(Engine& E, int count, const int* n, const double* dx, const double* const* phi,
+                         const esc_params* p, int prec) {
+  if (count < 1) return E.fail(ESC_EINVAL, "count must be >= 1");
+  if (!n || !dx || !phi || !p) return E.fail(ESC_EINVAL, "null argument");
+  if (prec != ESC_FP64 && prec != ESC_MIXED) return E.fail(ESC_EINVAL, "unknown precision");
+  for (int i = 0; i < count; ++i) {
+    if (!esc_supported_size(n[i]))
+      return E.fail(ESC_EINVAL, "unsupported grid size " + std::to_string(n[i]) +
+                                    " (need even n = 2^a 3^b, 8 <= n <= 4096)");
+    if (!(dx[i] > 0.0) || !std::isfinite(dx[i])) return E.fail(ESC_EINVAL, "spacing must be positive and finite");
+    if (!phi[i]) return E.fail(ESC_EINVAL, "null particle field");
+    if (!finite_params(p[i])) return E.fail(ESC_EINVAL, "non-finite model parameter");
+  }
+  CK(cudaGetDevice(&E.device));
+  E.count = count;
+  E.prec = prec;
+  E.n.assign(n, n + count);
+  E.dx.assign(dx, dx + count);
+  E.p.resize(count);
+  for (int i = 0; i < count; ++i) {
+    const esc_params& q = p[i];
+    E.p[i] = esc::ModelParams{q.A, q.B, q.chi, q.P, q.ca, q.cb, q.cc, q.kappa, q.mobility, q.Q};
+  }
+  std::map<int, int> gi;
+  E.where.resize(count);
+  for (int i = 0; i < count; ++i) {
+    auto it = gi.find(n[i]);
+    if (it == gi.end()) {
+      it = gi.emplace(n[i], (int)E.groups.size()).first;
+      E.groups.emplace_back();
+      E.groups.back().n = n[i];
+    }
+    Group& g = E.groups[it->second];
+    E.where[i] = {it->second, (int)g.members.size()};
+    g.members.push_back(i);
+  }
+  CK(cudaStreamCreateWithFlags(&E.own, cudaStreamNonBlocking));
+  E.stream = E.own;
+  TRY(E.alloc(&E.base, sizeof(int), "step counter"));
+  for (Group& g : E.groups) {
+    g.ks = find_kernels(g.n, prec);
+    if (!g.ks) return E.fail(ESC_EINVAL, "no kernels for n=" + std::to_string(g.n));
+    CK(g.ks->prepare());
+    const size_t cnt = g.members.size();
+    const size_t nn = (size_t)g.n * g.n;
+    const size_t sr = g.ks->sr_bytes, wr = g.ks->wr_bytes;
+    TRY(E.alloc(&g.S, cnt * nn * sr, "state buffer"));
+    TRY(E.alloc(&g.F, cnt * nn * wr, "f' buffer"));
+    TRY(E.alloc(&g.G, cnt * nn * 2 * wr, "flux buffer"));
+    TRY(E.alloc(&g.phi, cnt * nn * wr, "particle buffer"));
+    TRY(E.alloc(&g.tw_s, (size_t)g.n * 2 * sr, "twiddles"));
+    TRY(E.alloc(&g.tw_w, (size_t)g.n * 2 * wr, "twiddles"));
+    TRY(E.alloc(&g.cio, cnt * nn * sizeof(double), "field staging"));
+    TRY(E.alloc(&g.part, cnt * (size_t)g.ks->part_len * sizeof(double), "partials"));
+    TRY(E.alloc(&g.scal, cnt * 4 * sizeof(double), "scalars"));
+    TRY(E.alloc(&g.cnt, cnt * 4 * sizeof(unsigned), "counters"));
+    TRY(E.alloc(&g.status, cnt * sizeof(int), "status"));
+    TRY(E.alloc(&g.bad, cnt * sizeof(long long), "bad step"));
+    TRY(E.alloc(&g.d_inst, cnt * sizeof(esc::InstDev), "descriptors"));
+    // twiddles
+    if (sr == 8) {
+      auto t = twiddles<double>(g.n);
+      CK(cudaMemcpy(g.tw_s, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (wr == 8) {
+      auto t = twiddles<double>(g.n);
+      CK(cudaMemcpy(g.tw_w, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+      auto t = twiddles<float>(g.n);
+      CK(cudaMemcpy(g.tw_w, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    // particle fields in the work precision
+    if (wr == 8) {
+      for (size_t s = 0; s < cnt; ++s)
+        CK(cudaMemcpy(static_cast<double*>(g.phi) + s * nn, phi[g.members[s]], nn * sizeof(double),
+                      cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> tmp(nn);
+      for (size_t s = 0; s < cnt; ++s) {
+        const double* src = phi[g.members[s]];
+        for (size_t k = 0; k < nn; ++k) tmp[k] = (float)src[k];
+        CK(cudaMemcpy(static_cast<float*>(g.phi) + s * nn, tmp.data(), nn * sizeof(float),
+                      cudaMemcpyHostToDevice));
+      }
+    }
+    g.h_inst.resize(cnt);
+    for (size_t s = 0; s < cnt; ++s) {
+      esc::InstDev& d = g.h_inst[s];
+      memset(&d, 0, sizeof d);
+      const int i = g.members[s];
+      d.n = g.n;
+      d.dx = E.dx[i];
+      d.p = E.p[i];
+      d.S = static_cast<char*>(g.S) + s * nn * sr;
+      d.F = static_cast<char*>(g.F) + s * nn * wr;
+      d.G = static_cast<char*>(g.G) + s * nn * 2 * wr;
+      d.phi = static_cast<char*>(g.phi) + s * nn * wr;
+      d.part = g.part + s * (size_t)g.ks->part_len;
+      d.cnt = g.cnt + s * 4;
+      d.scal = g.scal + s * 4;
+      d.status = g.status + s;
+      d.bad_step = g.bad + s;
+      d.tw_s = g.tw_s;
+      d.tw_w = g.tw_w;
+      d.cio = g.cio + s * nn;
+    }
+    CK(cudaMemset(g.cnt, 0, cnt * 4 * sizeof(unsigned)));
+    CK(cudaMemset(g.status, 0, cnt * sizeof(int)));
+  }
+  CK(cudaDeviceSynchronize());
+  return ESC_OK;
+}
+
+// One step of every group: record history row (base + s_local) and advance.
+void launch_step(Engine& E, int s_local, cudaStream_t st) {
+  for (Group& g : E.groups) {
+    const int c = (int)g.members.size();
+    g.ks->row_a(g.d_inst, c, E.base, s_local, st);
+    g.ks->col_a(g.d_inst, c, E.base, s_local, st);
+    g.ks->row_b(g.d_inst, c, E.base, s_local, st);
+    g.ks->col_b(g.d_inst, c, st);
+  }
+}
+
+esc_status ensure_graph(Engine& E) {
+  if (E.gexec) return ESC_OK;
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(E.own, cudaStreamCaptureModeThreadLocal));
+  for (int s = 0; s < kChunk; ++s) launch_step(E, s, E.own);
+  k_advance<<<1, 32, 0, E.own>>>(E.base, kChunk);
+  const cudaError_t ec = cudaStreamEndCapture(E.own, &graph);
+  if (ec != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return E.fail_cuda("cudaStreamEndCapture", ec);
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&E.gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    E.gexec = nullptr;
+    return E.fail_cuda("cudaGraphInstantiate", ei);
+  }
+  return ESC_OK;
+}
+
+// c_in_out: per-instance pointers (host or device per `device_io`);
+// hist_host: per-instance host pointers (entries may be null) or null;
+// hist_dev: one device array for all instances or null.
+esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps, double dt,
+                      double* const* hist_host, double* hist_dev, int64_t* bad_out, bool leave_bad_unchanged) {
+  if (steps < 0) return E.fail(ESC_EINVAL, "steps must be >= 0");
+  if (!std::isfinite(dt)) return E.fail(ESC_EINVAL, "dt must be finite");
+  if (!cptr) return E.fail(ESC_EINVAL, "null composition array");
+  for (int i = 0; i < E.count; ++i)
+    if (!cptr[i]) return E.fail(ESC_EINVAL, "null composition field");
+  DeviceGuard dg(E.device);
+  const size_t rows = (size_t)steps + 1;
+  const size_t per = rows * 6;
+  double* hbase = hist_dev;
+  if (!hbase) {
+    const size_t need = per * (size_t)E.count;
+    if (need > E.hist_cap) {
+      if (E.hist) {
+        for (auto it = E.allocs.begin(); it != E.allocs.end(); ++it)
+          if (*it == E.hist) {
+            E.allocs.erase(it);
+            break;
+          }
+        cudaFree(E.hist);
+        E.hist = nullptr;
+        E.hist_cap = 0;
+      }
+      TRY(E.alloc(&E.hist, need * sizeof(double), "history"));
+      E.hist_cap = need;
+    }
+    hbase = E.hist;
+  }
+  cudaStream_t st = E.stream;
+  for (Group& g : E.groups) {
+    const size_t nn = (size_t)g.n * g.n;
+    for (size_t s = 0; s < g.members.size(); ++s) {
+      const int i = g.members[s];
+      esc::InstDev& d = g.h_inst[s];
+      d.dt = dt;
+      d.hist = hbase + (size_t)i * per;
+      d.hist_ld = (int)rows;
+      d.cio = device_io ? cptr[i] : g.cio + s * nn;
+    }
+    CK(cudaMemcpyAsync(g.d_inst, g.h_inst.data(), g.h_inst.size() * sizeof(esc::InstDev),
+                       cudaMemcpyHostToDevice, st));
+    if (!device_io) {
+      for (size_t s = 0; s < g.members.size(); ++s)
+        CK(cudaMemcpyAsync(g.cio + s * nn, cptr[g.members[s]], nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemsetAsync(g.status, 0, g.members.size() * sizeof(int), st));
+    CK(cudaMemsetAsync(g.bad, 0xff, g.members.size() * sizeof(long long), st));
+    CK(cudaMemsetAsync(g.cnt, 0, g.members.size() * 4 * sizeof(unsigned), st));
+  }
+  CK(cudaMemsetAsync(E.base, 0, sizeof(int), st));
+  for (Group& g : E.groups) g.ks->init(g.d_inst, (int)g.members.size(), st);
+  CK(cudaGetLastError());
+  int done = 0;
+  if (steps >= kChunk) {
+    TRY(ensure_graph(E));
+    while (steps - done >= kChunk) {
+      CK(cudaGraphLaunch(E.gexec, st));
+      done += kChunk;
+    }
+  }
+  const int rem = steps - done;
+  for (int s = 0; s < rem; ++s) launch_step(E, s, st);
+  if (rem) k_advance<<<1, 32, 0, st>>>(E.base, rem);
+  // history row `steps` of the final field (no update)
+  for (Group& g : E.groups) {
+    const int c = (int)g.members.size();
+    g.ks->row_a(g.d_inst, c, E.base, 0, st);
+    g.ks->col_a(g.d_inst, c, E.base, 0, st);
+    g.ks->row_b(g.d_inst, c, E.base, 0, st);
+  }
+  for (Group& g : E.groups) g.ks->fin(g.d_inst, (int)g.members.size(), st);
+  CK(cudaGetLastError());
+  // statuses
+  std::vector<int> status(E.count, 0);
+  std::vector<long long> bad(E.count, -1);
+  for (Group& g : E.groups) {
+    std::vector<int> s(g.members.size());
+    std::vector<long long> b(g.members.size());
+    CK(cudaMemcpyAsync(s.data(), g.status, s.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(b.data(), g.bad, b.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (size_t k = 0; k < g.members.size(); ++k) {
+      status[g.members[k]] = s[k];
+      bad[g.members[k]] = b[k];
+    }
+  }
+  bool any_bad = false;
+  for (int i = 0; i < E.count; ++i) {
+    if (status[i]) any_bad = true;
+    if (bad_out) bad_out[i] = status[i] ? (int64_t)bad[i] : -1;
+  }
+  if (!device_io) {
+    for (Group& g : E.groups) {
+      const size_t nn = (size_t)g.n * g.n;
+      for (size_t s = 0; s < g.members.size(); ++s) {
+        const int i = g.members[s];
+        if (status[i] && leave_bad_unchanged) continue;
+        CK(cudaMemcpyAsync(cptr[i], g.cio + s * nn, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+      }
+    }
+  }
+  if (hist_host) {
+    for (int i = 0; i < E.count; ++i)
+      if (hist_host[i])
+        CK(cudaMemcpyAsync(hist_host[i], hbase + (size_t)i * per, per * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  if (any_bad) {
+    for (int i = 0; i < E.count; ++i)
+      if (status[i])
+        return E.fail(ESC_ENONFINITE, "Non-finite composition at step " + std::to_string(bad[i]) +
+                                          (E.count > 1 ? " (instance " + std::to_string(i) + ")" : ""));
+  }
+  return ESC_OK;
+}
+
+}  // namespace
+
+struct esc_ctx {
+  Engine e;
+};
+struct esc_batch {
+  Engine e;
+};
+
+extern "C" {
+
+void esc_default_params(esc_params* p) {
+  if (!p) return;
+  p->A = 2.0;
+  p->B = 4.0;
+  p->chi = 0.5;
+  p->P = 5.0;
+  p->ca = 0.5;
+  p->cb = 0.0;
+  p->cc = 1.0;
+  p->kappa = 2.0;
+  p->mobility = 1.0;
+  p->Q = 0.5;
+}
+
+int esc_supported_size(int n) { return find_kernels(n, ESC_FP64) != nullptr ? 1 : 0; }
+
+const char* esc_version(void) { return "esc-b200 0.1.0 (sm_100a)"; }
+
+esc_status esc_create(esc_ctx** out, int n, double dx, const double* phi, const esc_params* p, esc_precision prec) {
+  if (!out) {
+    tl_err = "null output pointer";
+    return ESC_EINVAL;
+  }
+  *out = nullptr;
+  esc_ctx* c = new (std::nothrow) esc_ctx();
+  if (!c) {
+    tl_err = "host allocation failed";
+    return ESC_ENOMEM;
+  }
+  const double* phis[1] = {phi};
+  const esc_status s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
+  if (s != ESC_OK) {
+    tl_err = c->e.err;
+    c->e.release();
+    delete c;
+    return s;
+  }
+  *out = c;
+  return ESC_OK;
+}
+
+esc_status esc_run(esc_ctx* ctx, double* c, int steps, double dt, double* history, int64_t* bad_step) {
+  if (!ctx) {
+    tl_err = "null context";
+    return ESC_EINVAL;
+  }
+  double* cs[1] = {c};
+  double* hs[1] = {history};
+  int64_t b = -1;
+  const esc_status s = engine_run(ctx->e, cs, false, steps, dt, hs, nullptr, &b, true);
+  if (bad_step) *bad_step = b;
+  return s;
+}
+
+esc_status esc_run_device(esc_ctx* ctx, double* c, int steps, double dt, double* history, int64_t* bad_step) {
+  if (!ctx) {
+    tl_err = "null context";
+    return ESC_EINVAL;
+  }
+  double* cs[1] = {c};
+  int64_t b = -1;
+  const esc_status s = engine_run(ctx->e, cs, true, steps, dt, nullptr, history, &b, true);
+  if (bad_step) *bad_step = b;
+  return s;
+}
+
+esc_status esc_set_stream(esc_ctx* ctx, void* stream) {
+  if (!ctx) return ESC_EINVAL;
+  ctx->e.stream = stream ? static_cast<cudaStream_t>(stream) : ctx->e.own;
+  return ESC_OK;
+}
+
+const char* esc_last_error(const esc_ctx* ctx) { return ctx ? ctx->e.err.c_str() : tl_err.c_str(); }
+
+void esc_destroy(esc_ctx* ctx) {
+  if (!ctx) return;
+  {
+    DeviceGuard dg(ctx->e.device);
+    ctx->e.release();
+  }
+  delete ctx;
+}
+
+esc_status esc_batch_create(esc_batch** out, int count, const int* n, const double* dx, const double* const* phi,
+                            const esc_params* p, esc_precision prec) {
+  if (!out) {
+    tl_err = "null output pointer";
+    return ESC_EINVAL;
+  }
+  *out = nullptr;
+  esc_batch* b = new (std::nothrow) esc_batch();
+  if (!b) {
+    tl_err = "host allocation failed";
+    return ESC_ENOMEM;
+  }
+  const esc_status s = engine_create(b->e, count, n, dx, phi, p, (int)prec);
+  if (s != ESC_OK) {
+    tl_err = b->e.err;
+    b->e.release();
+    delete b;
+    return s;
+  }
+  *out = b;
+  return ESC_OK;
+}
+
+esc_status esc_batch_run(esc_batch* b, double* const* c, int steps, double dt, double* const* history,
+                         int64_t* bad_steps) {
+  if (!b) {
+    tl_err = "null batch";
+    return ESC_EINVAL;
+  }
+  return engine_run(b->e, c, false, steps, dt, history, nullptr, bad_steps, false);
+}
+
+esc_status esc_batch_run_device(esc_batch* b, double* const* c, int steps, double dt, double* history,
+                                int64_t* bad_steps) {
+  if (!b) {
+    tl_err = "null batch";
+    return ESC_EINVAL;
+  }
+  return engine_run(b->e, c, true, steps, dt, nullptr, history, bad_steps, false);
+}
+
+esc_status esc_batch_set_stream(esc_batch* b, void* stream) {
+  if (!b) return ESC_EINVAL;
+  b->e.stream = stream ? static_cast<cudaStream_t>(stream) : b->e.own;
+  return ESC_OK;
+}
+
+const char* esc_batch_last_error(const esc_batch* b) { return b ? b->e.err.c_str() : tl_err.c_str(); }
+
+void esc_batch_destroy(esc_batch* b) {
+  if (!b) return;
+  {
+    DeviceGuard dg(b->e.device);
+    b->e.release();
+  }
+  delete b;
+}
+
+}  // extern "C"

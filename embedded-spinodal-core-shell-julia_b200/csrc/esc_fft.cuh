@@ -1,0 +1,320 @@
+// In-register / shared-memory FFT engine for the Cahn-Hilliard stepper (sm_100a).
+//
+// One length-N complex DFT is computed by a group of T = N/E threads.  Thread t
+// of the group holds E values in registers, at positions t + T*m (m < E).  The
+// transform is a sequence of Stockham radix passes (radices R_0, R_1, ... with
+// product N, each dividing E): in every pass a thread performs E/R butterflies
+// whose inputs are exactly its own registers, so only the outputs of a
+// non-final pass are exchanged through shared memory (scatter, barrier,
+// gather, barrier).  The final pass writes back into the same registers, so the
+// result is again held at positions t + T*m in natural order.  A P-pass plan
+// therefore costs P-1 shared-memory exchanges and no staging of inputs or
+// outputs; the pointwise physics runs on the registers between transforms.
+//
+// The forward transform is the unnormalised DFT X(k) = sum_x x(x) e^{-2 pi i k x / N};
+// the inverse uses e^{+...} and is also unnormalised (callers fold 1/N into
+// their pointwise scale factors).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace esc {
+
+template <typename R>
+struct __align__(2 * sizeof(R)) cpx {
+  R x, y;
+};
+
+template <typename R>
+__device__ __forceinline__ cpx<R> mkc(R x, R y) {
+  cpx<R> c;
+  c.x = x;
+  c.y = y;
+  return c;
+}
+template <typename R>
+__device__ __forceinline__ cpx<R> operator+(cpx<R> a, cpx<R> b) { return mkc<R>(a.x + b.x, a.y + b.y); }
+template <typename R>
+__device__ __forceinline__ cpx<R> operator-(cpx<R> a, cpx<R> b) { return mkc<R>(a.x - b.x, a.y - b.y); }
+template <typename R>
+__device__ __forceinline__ cpx<R> cmul(cpx<R> a, cpx<R> b) {
+  return mkc<R>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+template <typename R>
+__device__ __forceinline__ cpx<R> cmulconj(cpx<R> a, cpx<R> b) {  // a * conj(b)
+  return mkc<R>(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
+}
+template <typename R>
+__device__ __forceinline__ cpx<R> cscale(cpx<R> a, R s) { return mkc<R>(a.x * s, a.y * s); }
+template <typename R>
+__device__ __forceinline__ cpx<R> cconj(cpx<R> a) { return mkc<R>(a.x, -a.y); }
+template <typename R>
+__device__ __forceinline__ cpx<R> times_i(cpx<R> a) { return mkc<R>(-a.y, a.x); }      // a * i
+template <typename R>
+__device__ __forceinline__ cpx<R> times_negi(cpx<R> a) { return mkc<R>(a.y, -a.x); }   // a * (-i)
+template <typename R, typename S>
+__device__ __forceinline__ cpx<R> ccast(cpx<S> a) { return mkc<R>((R)a.x, (R)a.y); }
+
+// read-only (non-coherent cache) load of a complex value
+template <typename R>
+__device__ __forceinline__ cpx<R> ldc(const cpx<R>* p);
+template <>
+__device__ __forceinline__ cpx<float> ldc<float>(const cpx<float>* p) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  return mkc<float>(v.x, v.y);
+}
+template <>
+__device__ __forceinline__ cpx<double> ldc<double>(const cpx<double>* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  return mkc<double>(v.x, v.y);
+}
+
+// cos / sin of 2*pi*a/48 for the multiples used by the in-register radices
+// (6, 8, 12, 16 all divide 48).  Correctly rounded double constants.
+__device__ __forceinline__ constexpr double cos48(int a) {
+  switch (((a % 48) + 48) % 48) {
+    case 0: return 1.0;
+    case 3: return 9.238795325112867384831e-01;
+    case 4: return 8.660254037844385965883e-01;
+    case 6: return 7.071067811865475727373e-01;
+    case 8: return 5.0e-01;
+    case 9: return 3.826834323650897817792e-01;
+    case 12: return 0.0;
+    case 15: return -3.826834323650897817792e-01;
+    case 16: return -5.0e-01;
+    case 18: return -7.071067811865475727373e-01;
+    case 20: return -8.660254037844385965883e-01;
+    case 21: return -9.238795325112867384831e-01;
+    case 24: return -1.0;
+    case 27: return -9.238795325112867384831e-01;
+    case 28: return -8.660254037844385965883e-01;
+    case 30: return -7.071067811865475727373e-01;
+    case 32: return -5.0e-01;
+    case 33: return -3.826834323650897817792e-01;
+    case 36: return 0.0;
+    case 39: return 3.826834323650897817792e-01;
+    case 40: return 5.0e-01;
+    case 42: return 7.071067811865475727373e-01;
+    case 44: return 8.660254037844385965883e-01;
+    case 45: return 9.238795325112867384831e-01;
+    default: return 0.0;  // not used by any radix
+  }
+}
+__device__ __forceinline__ constexpr double sin48(int a) { return cos48(a - 12); }
+
+// multiply by e^{sign * 2 pi i e / R}, sign = -1 forward, +1 inverse; e, R compile-time after unrolling
+template <int R, bool INV, typename Re>
+__device__ __forceinline__ cpx<Re> twiddle_const(cpx<Re> v, int e) {
+  e %= R;
+  if (e == 0) return v;
+  if (4 * e == R) return INV ? times_i(v) : times_negi(v);
+  if (2 * e == R) return mkc<Re>(-v.x, -v.y);
+  if (4 * e == 3 * R) return INV ? times_negi(v) : times_i(v);
+  const int a = e * (48 / R);
+  const Re c = (Re)cos48(a);
+  const Re s = INV ? (Re)sin48(a) : -(Re)sin48(a);
+  return mkc<Re>(fma(v.x, c, -v.y * s), fma(v.x, s, v.y * c));
+}
+
+// ---- small DFTs in registers -------------------------------------------------
+template <int R, bool INV, typename Re>
+struct DFT;
+
+template <bool INV, typename Re>
+struct DFT<2, INV, Re> {
+  static __device__ __forceinline__ void run(cpx<Re>* b) {
+    const cpx<Re> a0 = b[0], a1 = b[1];
+    b[0] = a0 + a1;
+    b[1] = a0 - a1;
+  }
+};
+
+template <bool INV, typename Re>
+struct DFT<3, INV, Re> {
+  static __device__ __forceinline__ void run(cpx<Re>* b) {
+    const Re h = (Re)8.660254037844385965883e-01;  // sqrt(3)/2
+    const cpx<Re> t1 = b[1] + b[2];
+    const cpx<Re> t2 = mkc<Re>(fma((Re)-0.5, t1.x, b[0].x), fma((Re)-0.5, t1.y, b[0].y));
+    const cpx<Re> d = b[1] - b[2];
+    // forward: X1 = t2 - i h d, X2 = t2 + i h d ; inverse swaps the sign of i
+    const cpx<Re> ihd = mkc<Re>(-h * d.y, h * d.x);  // i*h*d
+    b[0] = b[0] + t1;
+    if (INV) {
+      b[1] = t2 + ihd;
+      b[2] = t2 - ihd;
+    } else {
+      b[1] = t2 - ihd;
+      b[2] = t2 + ihd;
+    }
+  }
+};
+
+template <bool INV, typename Re>
+struct DFT<4, INV, Re> {
+  static __device__ __forceinline__ void run(cpx<Re>* b) {
+    const cpx<Re> s02 = b[0] + b[2], d02 = b[0] - b[2];
+    const cpx<Re> s13 = b[1] + b[3], d13 = b[1] - b[3];
+    const cpx<Re> r = INV ? times_i(d13) : times_negi(d13);
+    b[0] = s02 + s13;
+    b[2] = s02 - s13;
+    b[1] = d02 + r;
+    b[3] = d02 - r;
+  }
+};
+
+// composite DFT of size R1*R2 (input n = R2*n1 + n2, output k = k1 + R1*k2)
+template <int R1, int R2, bool INV, typename Re>
+__device__ __forceinline__ void dft_composite(cpx<Re>* b) {
+  constexpr int R = R1 * R2;
+  cpx<Re> y[R];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) {
+    cpx<Re> u[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) u[n1] = b[R2 * n1 + n2];
+    DFT<R1, INV, Re>::run(u);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) y[k1 * R2 + n2] = twiddle_const<R, INV>(u[k1], n2 * k1);
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < R1; ++k1) {
+    cpx<Re> u[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) u[n2] = y[k1 * R2 + n2];
+    DFT<R2, INV, Re>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) b[k1 + R1 * k2] = u[k2];
+  }
+}
+
+template <bool INV, typename Re>
+struct DFT<6, INV, Re> {
+  static __device__ __forceinline__ void run(cpx<Re>* b) { dft_composite<2, 3, INV, Re>(b); }
+};
+template <bool INV, typename Re>
+struct DFT<8, INV, Re> {
+  static __device__ __forceinline__ void run(cpx<Re>* b) { dft_composite<2, 4, INV, Re>(b); }
+};
+template <bool INV, typename Re>
+struct DFT<12, INV, Re> {
+  static __device__ __forceinline__ void run(cpx<Re>* b) { dft_composite<3, 4, INV, Re>(b); }
+};
+template <bool INV, typename Re>
+struct DFT<16, INV, Re> {
+  static __device__ __forceinline__ void run(cpx<Re>* b) { dft_composite<4, 4, INV, Re>(b); }
+};
+
+// ---- plans -------------------------------------------------------------------
+template <int... Rs>
+struct Radices {};
+
+template <int N_, int E_, typename RadList>
+struct Plan {
+  static constexpr int N = N_;
+  static constexpr int E = E_;
+  static constexpr int T = N_ / E_;
+  using List = RadList;
+};
+
+// Default plans: E elements per thread, radix sequence (each radix divides E).
+template <int N>
+struct DefaultPlan;
+#define ESC_PLAN(n, e, ...) \
+  template <>               \
+  struct DefaultPlan<n> { using type = Plan<n, e, Radices<__VA_ARGS__>>; };
+ESC_PLAN(8, 8, 8)
+ESC_PLAN(12, 12, 3, 4)
+ESC_PLAN(16, 16, 16)
+ESC_PLAN(24, 12, 3, 4, 2)
+ESC_PLAN(32, 8, 4, 8)
+ESC_PLAN(48, 12, 3, 4, 4)
+ESC_PLAN(64, 8, 8, 8)
+ESC_PLAN(96, 24, 3, 4, 8)
+ESC_PLAN(128, 16, 8, 16)
+ESC_PLAN(192, 12, 3, 4, 4, 4)
+ESC_PLAN(256, 16, 16, 16)
+ESC_PLAN(384, 24, 6, 8, 8)
+ESC_PLAN(512, 8, 8, 8, 8)
+ESC_PLAN(768, 24, 12, 8, 8)
+ESC_PLAN(1024, 16, 4, 16, 16)
+ESC_PLAN(1536, 24, 3, 8, 8, 8)
+ESC_PLAN(2048, 16, 8, 16, 16)
+ESC_PLAN(3072, 24, 6, 8, 8, 8)
+ESC_PLAN(4096, 16, 16, 16, 16)
+#undef ESC_PLAN
+
+// shared-memory padding: one element every 16
+__device__ __forceinline__ int smpad(int p) { return p + (p >> 4); }
+
+// Exchange addressing.  Row layout: group g owns a padded region of N elements;
+// Col layout: element p of column w sits at linear index p*W + w (then padded).
+template <int N>
+struct RowLayout {
+  int base;  // g * stride
+  static constexpr int stride = N + N / 16 + 1;
+  __device__ __forceinline__ int operator()(int p) const { return base + smpad(p); }
+};
+template <int W>
+struct ColLayout {
+  int w;
+  __device__ __forceinline__ int operator()(int p) const { return smpad(p * W + w); }
+};
+
+// One Stockham pass (radix RAD, NS = product of earlier radices).
+template <bool INV, class P, int RAD, int NS, bool LAST, typename Re, class L>
+__device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
+                                              const cpx<Re>* __restrict__ tw) {
+  constexpr int N = P::N, E = P::E, T = P::T;
+  constexpr int NB = E / RAD;
+  static_assert(E % RAD == 0, "radix must divide E");
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int j = t + T * q;
+    cpx<Re> b[RAD];
+#pragma unroll
+    for (int s = 0; s < RAD; ++s) b[s] = v[q + s * NB];
+    if (NS > 1) {
+      const int k = j % NS;
+      constexpr int STEP = N / (NS * RAD);
+#pragma unroll
+      for (int s = 1; s < RAD; ++s) {
+        const cpx<Re> w = ldc(tw + s * k * STEP);
+        b[s] = INV ? cmulconj(b[s], w) : cmul(b[s], w);
+      }
+    }
+    DFT<RAD, INV, Re>::run(b);
+    if (LAST) {
+#pragma unroll
+      for (int s = 0; s < RAD; ++s) v[q + s * NB] = b[s];
+    } else {
+      const int base = (j / NS) * NS * RAD + (j % NS);
+#pragma unroll
+      for (int s = 0; s < RAD; ++s) sm[lay(base + s * NS)] = b[s];
+    }
+  }
+  if (!LAST) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = sm[lay(t + T * m)];
+    __syncthreads();
+  }
+}
+
+template <bool INV, class P, int NS, typename Re, class L, int RAD, int... REST>
+__device__ __forceinline__ void fft_passes(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
+                                           const cpx<Re>* __restrict__ tw, Radices<RAD, REST...>) {
+  constexpr bool LAST = sizeof...(REST) == 0;
+  stockham_pass<INV, P, RAD, NS, LAST>(v, t, sm, lay, tw);
+  if constexpr (!LAST) fft_passes<INV, P, NS * RAD>(v, t, sm, lay, tw, Radices<REST...>{});
+}
+
+// Length-N DFT of the values v[m] at positions t + T*m; result in the same slots.
+// tw: table of e^{-2 pi i j / N}, j < N, in global memory (read through L1).
+// Every thread of the CTA must call this (it contains __syncthreads).
+template <bool INV, class P, typename Re, class L>
+__device__ __forceinline__ void fft(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
+                                    const cpx<Re>* __restrict__ tw) {
+  fft_passes<INV, P, 1>(v, t, sm, lay, tw, typename P::List{});
+}
+
+}  // namespace esc

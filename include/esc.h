@@ -1,0 +1,121 @@
+/* esc.h -- C ABI of the B200 Cahn-Hilliard stepper for embedded core-shell particles.
+ *
+ * This library replaces the body of the time loop of the reference Julia model
+ * (saswataiith/embedded-spinodal-core-shell-julia, core_shell.jl:84-103,
+ * `run_simulation`): per step it records the history row
+ * [s*dt, mean c, energy, min c, max c, dissipation] of the current field and
+ * then applies the stabilised semi-implicit Fourier update
+ * (core_shell.jl:72-76).  All work runs in hand-written sm_100a CUDA kernels on
+ * one GPU; there is no CPU fallback.
+ *
+ * Conventions
+ *   - Fields are n x n real arrays in the memory order of a Julia Matrix{Float64}
+ *     (column-major, dimension 1 = x contiguous); a C-ordered NumPy array a[y][x]
+ *     has the same bytes.
+ *   - history is (steps+1) x 6 Float64, column-major like Julia's
+ *     zeros(steps+1, 6): row s (0-based) at history[s + col*(steps+1)].
+ *   - All pointers are host memory unless a function name says `_device`.
+ *   - Supported grid sizes: even n = 2^a 3^b with 8 <= n <= 4096 (esc_supported_size).
+ *   - Functions return esc_status and never exit, abort or trap.  The message of
+ *     the last failure is available from esc_last_error / esc_batch_last_error.
+ *   - One context per host thread at a time; calls on a context are not re-entrant.
+ */
+#ifndef ESC_H
+#define ESC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Model constants: field-for-field the Julia `Parameters` struct, core_shell.jl:4-15
+ * (defaults A=2, B=4, chi=0.5, P=5, ca=0.5, cb=0, cc=1, kappa=2, mobility=1, Q=0.5). */
+typedef struct {
+  double A, B, chi, P, ca, cb, cc, kappa, mobility, Q;
+} esc_params;
+
+typedef enum {
+  ESC_OK = 0,
+  ESC_EINVAL = 1,      /* bad argument or unsupported grid size */
+  ESC_ECUDA = 2,       /* CUDA runtime error (message in esc_last_error) */
+  ESC_ENONFINITE = 3,  /* composition became non-finite (core_shell.jl:93); *bad_step holds s */
+  ESC_ETIMEOUT = 4,    /* a bounded device-side wait gave up */
+  ESC_ENOMEM = 5       /* device allocation failed */
+} esc_status;
+
+typedef enum {
+  ESC_FP64 = 0,  /* plain drop-in: every field, transform and reduction in FP64 */
+  ESC_MIXED = 1  /* FP64 state c, its transforms and all history reductions;
+                    FP32 for f'(c), mu, grad mu and flux transforms */
+} esc_precision;
+
+typedef struct esc_ctx esc_ctx;
+typedef struct esc_batch esc_batch;
+
+/* Fills `p` with the defaults of core_shell.jl:4-15. */
+void esc_default_params(esc_params *p);
+
+/* 1 if n is a supported grid size, else 0. */
+int esc_supported_size(int n);
+
+/* Library version string. */
+const char *esc_version(void);
+
+/* Creates a single-particle context: grid n x n with spacing dx, fixed particle
+ * field phi (n*n), model constants p.  Replaces make_grid + geometry
+ * (core_shell.jl:86-87, :17-25, :39-43). */
+esc_status esc_create(esc_ctx **out, int n, double dx, const double *phi, const esc_params *p,
+                      esc_precision prec);
+
+/* Runs `steps` steps from c (n*n, in/out) like run_simulation(c0, phi; dt, steps)
+ * (core_shell.jl:84-103): fills history ((steps+1) x 6, column-major; may be NULL)
+ * and overwrites c with the final field.  On a non-finite field returns
+ * ESC_ENONFINITE with *bad_step = s (the step whose row was being recorded, as in
+ * core_shell.jl:93); rows before s are valid and c is left unchanged.  Otherwise
+ * *bad_step = -1.  bad_step may be NULL. */
+esc_status esc_run(esc_ctx *ctx, double *c, int steps, double dt, double *history, int64_t *bad_step);
+
+/* Same as esc_run with c (n*n) and history ((steps+1)*6, may be NULL) in device
+ * memory.  The work is queued on the context's stream (esc_set_stream) and the
+ * call returns when it has finished. */
+esc_status esc_run_device(esc_ctx *ctx, double *c, int steps, double dt, double *history, int64_t *bad_step);
+
+/* Uses `stream` (a cudaStream_t) for all later work of the context; NULL restores
+ * the context's own stream. */
+esc_status esc_set_stream(esc_ctx *ctx, void *stream);
+
+/* Message of the last failure on ctx (ctx may be NULL: last failure of this thread). */
+const char *esc_last_error(const esc_ctx *ctx);
+
+void esc_destroy(esc_ctx *ctx);
+
+/* Batched ensemble: `count` independent particles with their own grid size n[i],
+ * spacing dx[i], particle phi[i] (n[i]^2) and constants p[i], advanced together
+ * (same dt, same step count).  Grid sizes may differ. */
+esc_status esc_batch_create(esc_batch **out, int count, const int *n, const double *dx,
+                            const double *const *phi, const esc_params *p, esc_precision prec);
+
+/* Runs all instances for `steps` steps.  c[i] (n[i]^2, in/out) and history[i]
+ * ((steps+1) x 6 each, entries may be NULL) are host arrays; bad_steps (count
+ * entries, may be NULL) receives -1 or the step at which instance i became
+ * non-finite.  Returns ESC_ENONFINITE if any instance did; the others still run
+ * to the end and their outputs are valid. */
+esc_status esc_batch_run(esc_batch *b, double *const *c, int steps, double dt, double *const *history,
+                         int64_t *bad_steps);
+
+/* Device-memory variant of esc_batch_run: c[i] are device pointers; history, if
+ * not NULL, is ONE device array of count*(steps+1)*6 doubles, instance i at
+ * offset i*(steps+1)*6. */
+esc_status esc_batch_run_device(esc_batch *b, double *const *c, int steps, double dt, double *history,
+                                int64_t *bad_steps);
+
+esc_status esc_batch_set_stream(esc_batch *b, void *stream);
+const char *esc_batch_last_error(const esc_batch *b);
+void esc_batch_destroy(esc_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ESC_H */
