@@ -556,6 +556,76 @@ esc_status esc_batch_run_device(esc_batch* b, double* const* c, int steps, doubl
   return engine_run(b->e, c, true, steps, dt, nullptr, history, bad_steps, false);
 }
 
+esc_status esc_batch_profile_phases(esc_batch* b, int steps, int* n_groups, int* group_n, int* group_count,
+                                    double* ms) {
+  if (!b || steps < 1 || !n_groups) {
+    tl_err = "bad argument";
+    return ESC_EINVAL;
+  }
+  Engine& E = b->e;
+  DeviceGuard dg(E.device);
+  const int ng = (int)E.groups.size();
+  *n_groups = ng;
+  if (!group_n || !group_count || !ms) return ESC_OK;
+  cudaStream_t st = E.stream;
+  // write history row 0 into the library's own buffer, never into caller memory
+  const size_t need = 6 * (size_t)E.count;
+  if (need > E.hist_cap) {
+    for (auto it = E.allocs.begin(); it != E.allocs.end(); ++it)
+      if (*it == E.hist) {
+        E.allocs.erase(it);
+        break;
+      }
+    if (E.hist) cudaFree(E.hist);
+    E.hist = nullptr;
+    E.hist_cap = 0;
+    TRY(E.alloc(&E.hist, need * sizeof(double), "history"));
+    E.hist_cap = need;
+  }
+  for (Group& g : E.groups) {
+    for (size_t s = 0; s < g.members.size(); ++s) {
+      g.h_inst[s].hist = E.hist + (size_t)g.members[s] * 6;
+      g.h_inst[s].hist_ld = 1;
+    }
+    CK(cudaMemcpyAsync(g.d_inst, g.h_inst.data(), g.h_inst.size() * sizeof(esc::InstDev),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(g.status, 0, g.members.size() * sizeof(int), st));
+  }
+  std::vector<cudaEvent_t> ev(4 * ng + 1);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  std::vector<double> acc(4 * (size_t)ng, 0.0);
+  for (int s = 0; s < steps; ++s) {
+    CK(cudaMemsetAsync(E.base, 0, sizeof(int), st));
+    for (int gi = 0; gi < ng; ++gi) {
+      Group& g = E.groups[gi];
+      const int c = (int)g.members.size();
+      CK(cudaEventRecord(ev[4 * gi], st));
+      g.ks->row_a(g.d_inst, c, E.base, 0, st);
+      CK(cudaEventRecord(ev[4 * gi + 1], st));
+      g.ks->col_a(g.d_inst, c, E.base, 0, st);
+      CK(cudaEventRecord(ev[4 * gi + 2], st));
+      g.ks->row_b(g.d_inst, c, E.base, 0, st);
+      CK(cudaEventRecord(ev[4 * gi + 3], st));
+      g.ks->col_b(g.d_inst, c, st);
+      CK(cudaEventRecord(gi + 1 < ng ? ev[4 * (gi + 1)] : ev[4 * ng], st));
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev[4 * ng]));
+    for (int k = 0; k < 4 * ng; ++k) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int gi = 0; gi < ng; ++gi) {
+    group_n[gi] = E.groups[gi].n;
+    group_count[gi] = (int)E.groups[gi].members.size();
+    for (int k = 0; k < 4; ++k) ms[4 * gi + k] = acc[4 * gi + k] / steps;
+  }
+  return ESC_OK;
+}
+
 esc_status esc_batch_set_stream(esc_batch* b, void* stream) {
   if (!b) return ESC_EINVAL;
   b->e.stream = stream ? static_cast<cudaStream_t>(stream) : b->e.own;

@@ -106,6 +106,9 @@ _SIGNATURES = [
     ("esc_batch_run_device", ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double,
                                             _vp, _i64p]),
     ("esc_batch_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("esc_batch_profile_phases", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                                _dp]),
     ("esc_batch_last_error", ctypes.c_char_p, [_vp]),
     ("esc_batch_destroy", None, [_vp]),
 ]
@@ -274,6 +277,22 @@ class Batch:
         if st not in (ESC_OK, ESC_ENONFINITE):
             _raise(st, self._err())
         return [int(b) for b in bad]
+
+    def profile_phases(self, steps: int = 5):
+        """Mean kernel time (ms) of each phase per size group on the current
+        device state: list of (n, count, [row_a, col_a, row_b, col_b])."""
+        lib = load_library()
+        ng = ctypes.c_int(0)
+        st = lib.esc_batch_profile_phases(self._h, int(steps), ctypes.byref(ng), None, None, None)
+        if st != ESC_OK:
+            _raise(st, self._err())
+        gn = (ctypes.c_int * ng.value)()
+        gc = (ctypes.c_int * ng.value)()
+        ms = np.zeros(4 * ng.value)
+        st = lib.esc_batch_profile_phases(self._h, int(steps), ctypes.byref(ng), gn, gc, _ptr(ms))
+        if st != ESC_OK:
+            _raise(st, self._err())
+        return [(int(gn[i]), int(gc[i]), [float(x) for x in ms[4 * i:4 * i + 4]]) for i in range(ng.value)]
 
     def set_stream(self, stream_ptr: int) -> None:
         st = load_library().esc_batch_set_stream(self._h, _vp(stream_ptr) if stream_ptr else None)

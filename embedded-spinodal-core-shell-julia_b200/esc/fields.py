@@ -1,0 +1,59 @@
+"""Host-side generators of particle fields and initial compositions.
+
+These build the inputs of a run: the tanh disc and initial composition of
+``initial_fields`` (reference core_shell.jl:27-37), an elliptical particle, and
+whole-field noise for ensembles.  Noise comes from NumPy's PCG64 with the given
+seed (Julia's MersenneTwister stream is not reproducible outside Julia); the
+distribution -- uniform in [-amplitude, amplitude), mean removed over the
+particle interior -- is the reference's.  Arrays are C-ordered ``a[y, x]``
+(the bytes of the column-major Julia matrix).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = ["particle_disc", "particle_ellipse", "interior_noise", "whole_field_noise", "initial_fields"]
+
+
+def _centred(n: int, spacing: float) -> np.ndarray:
+    # x = (i - 1 - n÷2) * spacing for Julia's 1-based i  (core_shell.jl:29)
+    return (np.arange(n) - n // 2) * spacing
+
+
+def particle_disc(n: int, spacing: float = 1.0, radius: float = 70.0, width: float = 4.0) -> np.ndarray:
+    """phi = 0.5 (1 - tanh((r - radius) / width)), centred on index n÷2 (core_shell.jl:29-30)."""
+    x = _centred(n, spacing)
+    r = np.hypot(x.reshape(1, n), x.reshape(n, 1))
+    return 0.5 * (1.0 - np.tanh((r - radius) / width))
+
+
+def particle_ellipse(n: int, a: float, b: float, width: float, spacing: float = 1.0) -> np.ndarray:
+    """phi = 0.5 (1 - tanh((sqrt((x b/a)^2 + y^2) - b) / width)); semi-axis a along x, b along y."""
+    x = _centred(n, spacing).reshape(1, n)
+    y = _centred(n, spacing).reshape(n, 1)
+    return 0.5 * (1.0 - np.tanh((np.sqrt((x * b / a) ** 2 + y ** 2) - b) / width))
+
+
+def interior_noise(phi: np.ndarray, seed: int, amplitude: float = 0.01, mean: float = 0.5) -> np.ndarray:
+    """c = mean everywhere plus, inside (phi >= 0.5), uniform noise with its
+    interior mean removed (core_shell.jl:31-35)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    noise = amplitude * (2.0 * rng.random(phi.shape) - 1.0)
+    inside = phi >= 0.5
+    c = np.full(phi.shape, mean, dtype=np.float64)
+    if inside.any():
+        noise = noise - noise[inside].mean()
+        c[inside] += noise[inside]
+    return c
+
+
+def whole_field_noise(n: int, seed: int, mean: float = 0.5, amplitude: float = 0.01) -> np.ndarray:
+    """c0 = mean + U(-amplitude, amplitude) on every point."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return mean + amplitude * (2.0 * rng.random((n, n)) - 1.0)
+
+
+def initial_fields(n: int, spacing: float = 1.0, radius: float = 70.0, width: float = 4.0, seed: int = 5749):
+    """``initial_fields`` of core_shell.jl:27-37: returns (c, phi)."""
+    phi = particle_disc(n, spacing, radius, width)
+    return interior_noise(phi, seed), phi

@@ -111,6 +111,15 @@ esc_status esc_batch_run_device(esc_batch *b, double *const *c, int steps, doubl
                                 int64_t *bad_steps);
 
 esc_status esc_batch_set_stream(esc_batch *b, void *stream);
+
+/* Measurement aid: runs `steps` further steps on the batch's current device state
+ * (left by the last run) launching each phase kernel separately between CUDA
+ * events, and reports the mean duration in milliseconds of the four phase
+ * kernels (row A, column A, row B, column B) of every size group:
+ * ms[4*g + phase].  *n_groups receives the number of groups; call first with
+ * the arrays NULL to size them.  The history buffer row 0 is overwritten. */
+esc_status esc_batch_profile_phases(esc_batch *b, int steps, int *n_groups, int *group_n, int *group_count,
+                                    double *ms);
 const char *esc_batch_last_error(const esc_batch *b);
 void esc_batch_destroy(esc_batch *b);
 
