@@ -423,6 +423,9 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
 
 }  // namespace
 
+// Lets other translation units of the library report through esc_last_error(NULL).
+void esc_set_thread_error(const char* msg) { tl_err = msg ? msg : ""; }
+
 struct esc_ctx {
   Engine e;
 };

@@ -121,6 +121,23 @@ esc_status esc_batch_set_stream(esc_batch *b, void *stream);
 esc_status esc_batch_profile_phases(esc_batch *b, int steps, int *n_groups, int *group_n, int *group_count,
                                     double *ms);
 const char *esc_batch_last_error(const esc_batch *b);
+
+/* Allocation-free single-particle run.  No counterpart in the reference: it
+ * exists for callers that may not call cudaMalloc themselves or through this
+ * library (device memory owned by another allocator or a fixed budget, or a
+ * loop that cannot take the device-wide synchronisation of cudaMalloc/cudaFree).
+ * Inputs and outputs are caller-owned DEVICE buffers: phi (n*n), c (n*n, in/out),
+ * history ((steps+1) x 6 column-major, may be NULL).  FP64 only, same results as
+ * esc_run_device.  Every intermediate lives in one fixed __device__ array of the
+ * library (about 2.1 MiB per GPU, held until exit), so n is limited to 256:
+ * larger n returns ESC_EINVAL.  All calls share that array: calls that overlap on
+ * the GPU race and must be serialised by the caller.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Work is queued on `stream` (a cudaStream_t, NULL = default
+ * stream) and the call returns when it has finished.  Failures are described by
+ * esc_last_error(NULL). */
+esc_status esc_run_noalloc(int n, double dx, const double *phi, const esc_params *p, double *c, int steps,
+                           double dt, double *history, int64_t *bad_step, void *stream);
 void esc_batch_destroy(esc_batch *b);
 
 #ifdef __cplusplus
