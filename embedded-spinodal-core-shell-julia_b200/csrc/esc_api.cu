@@ -7,9 +7,12 @@
 // launch per group whose grid is (tiles, instances).  Steps are replayed from a
 // captured CUDA graph of kChunk steps; a device-side step counter gives each
 // launch its history row, so the graph never needs re-instantiation.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -63,7 +66,58 @@ struct Group {
   long long* bad = nullptr;
   esc::InstDev* d_inst = nullptr;
   std::vector<esc::InstDev> h_inst;
+  esc::ColMaps maps;      // tensor maps of S, F, G for the pipelined column kernels
+  bool pipe_rows = false;  // use the persistent TMA-fed row kernels
+  bool warp_rows = false;  // use the warp-independent row kernels
+  bool pipe_cols = false;  // use the persistent TMA-fed column kernels
 };
+
+// cuTensorMapEncodeTiled from the driver, looked up once
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 3-D map over `count` instances of n rows of `row_scalars` scalars; box = (box_x, RB, 1)
+bool encode_map(CUtensorMap* map, void* base, size_t scalar_bytes, int row_scalars, int rows, int count, int box_x,
+                int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const CUtensorMapDataType dt = scalar_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[3] = {(cuuint64_t)row_scalars, (cuuint64_t)rows, (cuuint64_t)count};
+  const cuuint64_t strides[2] = {(cuuint64_t)row_scalars * scalar_bytes,
+                                 (cuuint64_t)row_scalars * scalar_bytes * (cuuint64_t)rows};
+  const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+bool pipeline_enabled() {
+  const char* v = getenv("ESC_PIPE");
+  return !(v && v[0] == '0');
+}
+
+// ESC_ROWS = warp | pipe | legacy forces one row-kernel family (measurement aid)
+int row_family_override() {
+  const char* v = getenv("ESC_ROWS");
+  if (!v) return -1;
+  if (!strcmp(v, "legacy")) return 0;
+  if (!strcmp(v, "pipe")) return 1;
+  if (!strcmp(v, "warp")) return 2;
+  return -1;
+}
 
 struct Engine {
   int count = 0;
@@ -265,19 +319,69 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
     }
     CK(cudaMemset(g.cnt, 0, cnt * 4 * sizeof(unsigned)));
     CK(cudaMemset(g.status, 0, cnt * sizeof(int)));
+    if (g.ks->warp_rows) {
+      CK(g.ks->prepare_warp());
+      g.warp_rows = true;
+    }
+    if (pipeline_enabled()) {
+      CK(g.ks->prepare_pipe());
+      g.pipe_rows = g.ks->pipe_rows;
+      if (g.ks->pipe_cols) {
+        const int H = g.n / 2, W = g.ks->W, RB = g.ks->RB;
+        g.pipe_cols = encode_map(&g.maps.S, g.S, sr, 2 * H, g.n, (int)cnt, 2 * W, RB) &&
+                      encode_map(&g.maps.F, g.F, wr, 2 * H, g.n, (int)cnt, 2 * W, RB) &&
+                      encode_map(&g.maps.G, g.G, wr, 4 * H, g.n, (int)cnt, 4 * W, RB);
+      }
+    }
+    const int rf = row_family_override();
+    if (rf == 0) g.pipe_rows = g.warp_rows = false;
+    if (rf == 1) g.warp_rows = false;
+    if (rf == 2 && g.warp_rows) g.pipe_rows = false;
   }
   CK(cudaDeviceSynchronize());
   return ESC_OK;
 }
 
 // One step of every group: record history row (base + s_local) and advance.
+void phase_row_a(Group& g, const int* base, int s_local, cudaStream_t st) {
+  const int c = (int)g.members.size();
+  if (g.warp_rows)
+    g.ks->row_a_w(g.d_inst, c, base, s_local, st);
+  else if (g.pipe_rows)
+    g.ks->row_a_p(g.d_inst, c, base, s_local, st);
+  else
+    g.ks->row_a(g.d_inst, c, base, s_local, st);
+}
+void phase_col_a(Group& g, const int* base, int s_local, cudaStream_t st) {
+  const int c = (int)g.members.size();
+  if (g.pipe_cols)
+    g.ks->col_a_p(g.d_inst, c, base, s_local, st, &g.maps);
+  else
+    g.ks->col_a(g.d_inst, c, base, s_local, st);
+}
+void phase_row_b(Group& g, const int* base, int s_local, cudaStream_t st) {
+  const int c = (int)g.members.size();
+  if (g.warp_rows)
+    g.ks->row_b_w(g.d_inst, c, base, s_local, st);
+  else if (g.pipe_rows)
+    g.ks->row_b_p(g.d_inst, c, base, s_local, st);
+  else
+    g.ks->row_b(g.d_inst, c, base, s_local, st);
+}
+void phase_col_b(Group& g, cudaStream_t st) {
+  const int c = (int)g.members.size();
+  if (g.pipe_cols)
+    g.ks->col_b_p(g.d_inst, c, st, &g.maps);
+  else
+    g.ks->col_b(g.d_inst, c, st);
+}
+
 void launch_step(Engine& E, int s_local, cudaStream_t st) {
   for (Group& g : E.groups) {
-    const int c = (int)g.members.size();
-    g.ks->row_a(g.d_inst, c, E.base, s_local, st);
-    g.ks->col_a(g.d_inst, c, E.base, s_local, st);
-    g.ks->row_b(g.d_inst, c, E.base, s_local, st);
-    g.ks->col_b(g.d_inst, c, st);
+    phase_row_a(g, E.base, s_local, st);
+    phase_col_a(g, E.base, s_local, st);
+    phase_row_b(g, E.base, s_local, st);
+    phase_col_b(g, st);
   }
 }
 
@@ -370,10 +474,9 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
   if (rem) k_advance<<<1, 32, 0, st>>>(E.base, rem);
   // history row `steps` of the final field (no update)
   for (Group& g : E.groups) {
-    const int c = (int)g.members.size();
-    g.ks->row_a(g.d_inst, c, E.base, 0, st);
-    g.ks->col_a(g.d_inst, c, E.base, 0, st);
-    g.ks->row_b(g.d_inst, c, E.base, 0, st);
+    phase_row_a(g, E.base, 0, st);
+    phase_col_a(g, E.base, 0, st);
+    phase_row_b(g, E.base, 0, st);
   }
   for (Group& g : E.groups) g.ks->fin(g.d_inst, (int)g.members.size(), st);
   CK(cudaGetLastError());
@@ -413,6 +516,12 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
   }
   CK(cudaStreamSynchronize(st));
   if (any_bad) {
+    for (int i = 0; i < E.count; ++i)
+      if (status[i] == esc::kStatusLayout)
+        return E.fail(ESC_ECUDA, "internal error: a shared-memory stage was misaligned; no copy was issued");
+    for (int i = 0; i < E.count; ++i)
+      if (status[i] == esc::kStatusTimeout)
+        return E.fail(ESC_ETIMEOUT, "a bounded wait for a tile copy gave up (instance " + std::to_string(i) + ")");
     for (int i = 0; i < E.count; ++i)
       if (status[i])
         return E.fail(ESC_ENONFINITE, "Non-finite composition at step " + std::to_string(bad[i]) +
@@ -602,14 +711,15 @@ esc_status esc_batch_profile_phases(esc_batch* b, int steps, int* n_groups, int*
     for (int gi = 0; gi < ng; ++gi) {
       Group& g = E.groups[gi];
       const int c = (int)g.members.size();
+      (void)c;
       CK(cudaEventRecord(ev[4 * gi], st));
-      g.ks->row_a(g.d_inst, c, E.base, 0, st);
+      phase_row_a(g, E.base, 0, st);
       CK(cudaEventRecord(ev[4 * gi + 1], st));
-      g.ks->col_a(g.d_inst, c, E.base, 0, st);
+      phase_col_a(g, E.base, 0, st);
       CK(cudaEventRecord(ev[4 * gi + 2], st));
-      g.ks->row_b(g.d_inst, c, E.base, 0, st);
+      phase_row_b(g, E.base, 0, st);
       CK(cudaEventRecord(ev[4 * gi + 3], st));
-      g.ks->col_b(g.d_inst, c, st);
+      phase_col_b(g, st);
       CK(cudaEventRecord(gi + 1 < ng ? ev[4 * (gi + 1)] : ev[4 * ng], st));
     }
     CK(cudaGetLastError());

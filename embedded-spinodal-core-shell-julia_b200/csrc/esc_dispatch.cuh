@@ -1,7 +1,7 @@
 // Per-size kernel sets: launch wrappers and launch geometry for one grid size n
 // and one precision mode.  Each esc_size_<n>.cu instantiates the two modes.
 #pragma once
-#include "esc_kernels.cuh"
+#include "esc_warp.cuh"
 
 namespace esc {
 
@@ -14,12 +14,25 @@ struct KernelSet {
   size_t smem;   // dynamic shared memory per block
   size_t sr_bytes, wr_bytes;  // sizeof(real) of the state and work types
   cudaError_t (*prepare)();
+  cudaError_t (*prepare_pipe)();
   void (*init)(const InstDev*, int, cudaStream_t);
   void (*fin)(const InstDev*, int, cudaStream_t);
   void (*row_a)(const InstDev*, int, const int*, int, cudaStream_t);
   void (*col_a)(const InstDev*, int, const int*, int, cudaStream_t);
   void (*row_b)(const InstDev*, int, const int*, int, cudaStream_t);
   void (*col_b)(const InstDev*, int, cudaStream_t);
+  // persistent TMA-fed launchers (available when pipe_rows / pipe_cols)
+  bool pipe_rows, pipe_cols;
+  int W, RB;  // columns per tile and rows per tensor box of the column kernels
+  void (*row_a_p)(const InstDev*, int, const int*, int, cudaStream_t);
+  void (*row_b_p)(const InstDev*, int, const int*, int, cudaStream_t);
+  void (*col_a_p)(const InstDev*, int, const int*, int, cudaStream_t, const ColMaps*);
+  void (*col_b_p)(const InstDev*, int, cudaStream_t, const ColMaps*);
+  // warp-independent row kernels (groups inside one warp), when warp_rows
+  bool warp_rows;
+  void (*row_a_w)(const InstDev*, int, const int*, int, cudaStream_t);
+  void (*row_b_w)(const InstDev*, int, const int*, int, cudaStream_t);
+  cudaError_t (*prepare_warp)();
 };
 
 // FP64 plans keep E <= 16 so that two register arrays of double2 fit.
@@ -86,6 +99,115 @@ struct KS {
   static void col_b(const InstDev* d, int count, cudaStream_t st) {
     k_col_b<P, SR, WR><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(d);
   }
+  using PG = PipeGeom<P, SR, WR>;
+  // occupancy (blocks per SM) of the persistent kernels and the SM count, set by prepare()
+  static int& occ(int i) {
+    static int v[4] = {1, 1, 1, 1};
+    return v[i];
+  }
+  static int& sms() {
+    static int v = 148;
+    return v;
+  }
+  static int grid_for(int total, int which) {
+    const int cap = occ(which) * sms();
+    return total < cap ? total : cap;
+  }
+  static cudaError_t prepare_pipe() {
+    cudaError_t e;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev))) return e;
+    if ((e = cudaDeviceGetAttribute(&sms(), cudaDevAttrMultiProcessorCount, dev))) return e;
+    if constexpr (PG::row_ok) {
+      const int ba = (int)(2 * PG::stage_ra + kStageAlignSlack), bb = (int)(2 * PG::stage_rb + kStageAlignSlack);
+      if ((e = cudaFuncSetAttribute(k_row_a_p<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ba)))
+        return e;
+      if ((e = cudaFuncSetAttribute(k_row_b_p<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bb)))
+        return e;
+      if ((e = cudaFuncSetAttribute(k_row_a_p<P, SR, WR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared)))
+        return e;
+      if ((e = cudaFuncSetAttribute(k_row_b_p<P, SR, WR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared)))
+        return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ(0), k_row_a_p<P, SR, WR>, kBlock, ba))) return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ(2), k_row_b_p<P, SR, WR>, kBlock, bb))) return e;
+    }
+    if constexpr (PG::col_ok) {
+      const int ba = (int)(2 * PG::stage_ca + kStageAlignSlack), bb = (int)(2 * PG::stage_cb + kStageAlignSlack);
+      if ((e = cudaFuncSetAttribute(k_col_a_p<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ba)))
+        return e;
+      if ((e = cudaFuncSetAttribute(k_col_b_p<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bb)))
+        return e;
+      if ((e = cudaFuncSetAttribute(k_col_a_p<P, SR, WR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared)))
+        return e;
+      if ((e = cudaFuncSetAttribute(k_col_b_p<P, SR, WR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared)))
+        return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ(1), k_col_a_p<P, SR, WR>, PG::CB, ba))) return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ(3), k_col_b_p<P, SR, WR>, PG::CB, bb))) return e;
+    }
+    for (int i = 0; i < 4; ++i)
+      if (occ(i) < 1) occ(i) = 1;
+    return cudaSuccess;
+  }
+  static void row_a_p(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
+    if constexpr (PG::row_ok) {
+      const int total = count * tiles_pairs;
+      k_row_a_p<P, SR, WR><<<grid_for(total, 0), kBlock, 2 * PG::stage_ra + kStageAlignSlack, st>>>(d, count, base, s);
+    }
+  }
+  static void row_b_p(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
+    if constexpr (PG::row_ok) {
+      const int total = count * tiles_rows;
+      k_row_b_p<P, SR, WR><<<grid_for(total, 2), kBlock, 2 * PG::stage_rb + kStageAlignSlack, st>>>(d, count, base, s);
+    }
+  }
+  static void col_a_p(const InstDev* d, int count, const int* base, int s, cudaStream_t st, const ColMaps* m) {
+    if constexpr (PG::col_ok) {
+      const int total = count * PG::tiles_cols;
+      k_col_a_p<P, SR, WR><<<grid_for(total, 1), PG::CB, 2 * PG::stage_ca + kStageAlignSlack, st>>>(d, count, base, s, *m);
+    }
+  }
+  static void col_b_p(const InstDev* d, int count, cudaStream_t st, const ColMaps* m) {
+    if constexpr (PG::col_ok) {
+      const int total = count * PG::tiles_cols;
+      k_col_b_p<P, SR, WR><<<grid_for(total, 3), PG::CB, 2 * PG::stage_cb + kStageAlignSlack, st>>>(d, count, *m);
+    }
+  }
+  // ---- warp-independent rows (their own plan, groups inside one warp) ----
+  using WP = typename WarpPlan<N>::type;
+  static constexpr bool warp_ok = (WP::T <= 32) && (32 % WP::T == 0);
+  static size_t warp_smem() {
+    if constexpr (warp_ok) return WarpRowGeom<WP>::template smem<SR>();
+    return 0;
+  }
+  static int warp_tiles_pairs() {
+    if constexpr (warp_ok) return WarpRowGeom<WP>::tiles_pairs;
+    return 0;
+  }
+  static int warp_tiles_rows() {
+    if constexpr (warp_ok) return WarpRowGeom<WP>::tiles_rows;
+    return 0;
+  }
+  static cudaError_t prepare_warp() {
+    if constexpr (warp_ok) {
+      cudaError_t e;
+      const int b = (int)warp_smem();
+      if ((e = cudaFuncSetAttribute(k_row_a_w<WP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+      if ((e = cudaFuncSetAttribute(k_row_b_w<WP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    }
+    return cudaSuccess;
+  }
+  static void row_a_w(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
+    if constexpr (warp_ok)
+      k_row_a_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kBlock, warp_smem(), st>>>(d, base, s);
+  }
+  static void row_b_w(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
+    if constexpr (warp_ok)
+      k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kBlock, warp_smem(), st>>>(d, base, s);
+  }
   static KernelSet make(int prec) {
     KernelSet k;
     k.n = N;
@@ -95,7 +217,14 @@ struct KS {
     k.tiles_pairs = tiles_pairs;
     k.tiles_rows = tiles_rows;
     k.tiles_cols = tiles_cols;
-    k.part_len = 5 * tiles_pairs + tiles_cols + tiles_rows;
+    {
+      // partial sums are scratch of one launch; size for the largest user
+      int need = 5 * tiles_pairs + (tiles_cols > PG::tiles_cols ? tiles_cols : PG::tiles_cols) + tiles_rows;
+      const int wa = 5 * warp_tiles_pairs() * (kBlock / 32), wb = warp_tiles_rows() * (kBlock / 32);
+      if (wa > need) need = wa;
+      if (wb > need) need = wb;
+      k.part_len = need;
+    }
     k.smem = smem();
     k.sr_bytes = sizeof(SR);
     k.wr_bytes = sizeof(WR);
@@ -106,6 +235,19 @@ struct KS {
     k.col_a = &col_a;
     k.row_b = &row_b;
     k.col_b = &col_b;
+    k.pipe_rows = PG::row_ok;
+    k.pipe_cols = PG::col_ok;
+    k.W = PG::W;
+    k.RB = PG::RB;
+    k.row_a_p = &row_a_p;
+    k.row_b_p = &row_b_p;
+    k.col_a_p = &col_a_p;
+    k.col_b_p = &col_b_p;
+    k.prepare_pipe = &prepare_pipe;
+    k.warp_rows = warp_ok;
+    k.row_a_w = &row_a_w;
+    k.row_b_w = &row_b_w;
+    k.prepare_warp = &prepare_warp;
     return k;
   }
 };

@@ -260,8 +260,17 @@ struct ColLayout {
   __device__ __forceinline__ int operator()(int p) const { return smpad(p * W + w); }
 };
 
+// Barrier used between the scatter and gather of an exchange: the whole block,
+// or only the warp when every FFT group lives inside one warp.
+struct BlockSync {
+  static __device__ __forceinline__ void sync() { __syncthreads(); }
+};
+struct WarpSync {
+  static __device__ __forceinline__ void sync() { __syncwarp(); }
+};
+
 // One Stockham pass (radix RAD, NS = product of earlier radices).
-template <bool INV, class P, int RAD, int NS, bool LAST, typename Re, class L>
+template <bool INV, class P, int RAD, int NS, bool LAST, class Sync = BlockSync, typename Re, class L>
 __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
                                               const cpx<Re>* __restrict__ tw) {
   constexpr int N = P::N, E = P::E, T = P::T;
@@ -293,28 +302,46 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
     }
   }
   if (!LAST) {
-    __syncthreads();
+    Sync::sync();
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = sm[lay(t + T * m)];
-    __syncthreads();
+    Sync::sync();
   }
 }
 
-template <bool INV, class P, int NS, typename Re, class L, int RAD, int... REST>
+template <bool INV, class P, int NS, class Sync, typename Re, class L, int RAD, int... REST>
 __device__ __forceinline__ void fft_passes(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
                                            const cpx<Re>* __restrict__ tw, Radices<RAD, REST...>) {
   constexpr bool LAST = sizeof...(REST) == 0;
-  stockham_pass<INV, P, RAD, NS, LAST>(v, t, sm, lay, tw);
-  if constexpr (!LAST) fft_passes<INV, P, NS * RAD>(v, t, sm, lay, tw, Radices<REST...>{});
+  stockham_pass<INV, P, RAD, NS, LAST, Sync>(v, t, sm, lay, tw);
+  if constexpr (!LAST) fft_passes<INV, P, NS * RAD, Sync>(v, t, sm, lay, tw, Radices<REST...>{});
 }
 
 // Length-N DFT of the values v[m] at positions t + T*m; result in the same slots.
 // tw: table of e^{-2 pi i j / N}, j < N, in global memory (read through L1).
 // Every thread of the CTA must call this (it contains __syncthreads).
-template <bool INV, class P, typename Re, class L>
+template <bool INV, class P, class Sync = BlockSync, typename Re, class L>
 __device__ __forceinline__ void fft(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
                                     const cpx<Re>* __restrict__ tw) {
-  fft_passes<INV, P, 1>(v, t, sm, lay, tw, typename P::List{});
+  fft_passes<INV, P, 1, Sync>(v, t, sm, lay, tw, typename P::List{});
 }
+
+// Exchange layout of one warp-local FFT group: n elements at `base`, XOR
+// swizzled inside each 128-byte line (with a per-group offset) so that the
+// strided scatters and the gathers of one warp hit distinct banks.  Requires
+// n to be a multiple of the line length; smaller or odd sizes stay linear.
+template <int N, int ELEM_BYTES>
+struct SwizzleLayout {
+  int base;
+  int g;  // group index inside the warp
+  static constexpr int LINE = 128 / ELEM_BYTES;  // elements per 128-byte line
+  __device__ __forceinline__ int operator()(int p) const {
+    if constexpr (N % LINE == 0) {
+      return base + (p ^ (((p / LINE) + 4 * g) & (LINE - 1)));
+    } else {
+      return base + p;
+    }
+  }
+};
 
 }  // namespace esc

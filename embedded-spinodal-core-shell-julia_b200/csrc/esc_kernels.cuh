@@ -83,7 +83,7 @@ __device__ __forceinline__ double block_reduce(double v, double* red) {
   if (lane == 0) red[wid] = v;
   __syncthreads();
   if (wid == 0) {
-    v = (lane < kBlock / 32) ? red[lane] : Op::identity();
+    v = (lane < (int)(blockDim.x >> 5)) ? red[lane] : Op::identity();
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = Op::ap(v, __shfl_xor_sync(0xffffffffu, v, o));
   }
@@ -115,7 +115,7 @@ template <class Op>
 __device__ __forceinline__ double reduce_partials(const double* p, int count, int stride, double init,
                                                   double* red) {
   double v = init;
-  for (int i = threadIdx.x; i < count; i += kBlock) v = Op::ap(v, __ldcg(p + (size_t)i * stride));
+  for (int i = threadIdx.x; i < count; i += blockDim.x) v = Op::ap(v, __ldcg(p + (size_t)i * stride));
   return block_reduce<Op>(v, red);
 }
 

@@ -1,0 +1,267 @@
+// Warp-independent row kernels (row A and row B).
+//
+// Every FFT group (T <= 32 threads, one row pair for row A, one row for row B)
+// lives inside a single warp and exchanges through its own swizzled slice of
+// shared memory, so the transforms need only __syncwarp.  History partials are
+// reduced per warp and the last warp to arrive for an instance folds them.
+// No block-wide barrier remains: the warps of a block drift freely, and one
+// warp's global loads overlap another warp's transforms.  The numerics are
+// those of k_row_a / k_row_b in esc_kernels.cuh, operation for operation.
+#pragma once
+#include "esc_pipe.cuh"
+
+namespace esc {
+
+// Plans with every group inside a warp (T <= 32) and E <= 16 where possible.
+template <int N>
+struct WarpPlan {
+  using type = typename DefaultPlan<N>::type;
+};
+#define ESC_WPLAN(n, e, ...) \
+  template <>                \
+  struct WarpPlan<n> { using type = Plan<n, e, Radices<__VA_ARGS__>>; };
+ESC_WPLAN(96, 12, 6, 4, 4)
+ESC_WPLAN(384, 12, 6, 4, 4, 4)
+ESC_WPLAN(512, 16, 16, 16, 2)
+ESC_WPLAN(768, 24, 12, 8, 8)
+#undef ESC_WPLAN
+
+template <class P>
+struct WarpRowGeom {
+  static constexpr int N = P::N, T = P::T, H = N / 2;
+  static_assert(T <= 32 && 32 % T == 0, "warp kernels need groups inside one warp");
+  static constexpr int GPW = 32 / T;            // groups per warp
+  static constexpr int NW = kBlock / 32;        // warps per block
+  static constexpr int G = GPW * NW;            // groups per block
+  static constexpr int tiles_pairs = (H + G - 1) / G;
+  static constexpr int tiles_rows = (N + G - 1) / G;
+  template <typename SR>
+  static constexpr size_t smem() {
+    return (size_t)G * N * sizeof(cpx<SR>);
+  }
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Warp-level arrival: returns true (in every lane) in the warp that arrives
+// last among `total` arrivals; its earlier partial writes are then visible.
+__device__ __forceinline__ bool warp_arrive_last(unsigned* counter, unsigned total) {
+  unsigned last = 0;
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == total - 1) ? 1u : 0u;
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (last) __threadfence();
+  return last != 0;
+}
+
+// deterministic warp fold of `count` partials spaced `stride` apart
+template <class Op>
+__device__ __forceinline__ double warp_fold(const double* p, int count, int stride, double init) {
+  double v = init;
+  for (int i = (threadIdx.x & 31); i < count; i += 32) v = Op::ap(v, __ldcg(p + (size_t)i * stride));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = Op::ap(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ bool warp_instance_running(const int* status) {
+  int s = 0;
+  if ((threadIdx.x & 31) == 0) s = *(volatile const int*)status;
+  return __shfl_sync(0xffffffffu, s, 0) == 0;
+}
+
+// =====================================================================================
+template <class P, typename SR, typename WR>
+__global__ void __launch_bounds__(kBlock, 2) k_row_a_w(const InstDev* __restrict__ insts,
+                                                       const int* __restrict__ base, int s_local) {
+  using WG = WarpRowGeom<P>;
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
+  constexpr int tiles = WG::tiles_pairs;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const InstDev& I = insts[blockIdx.y];
+  if (!warp_instance_running(I.status)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = lane % T, gw = lane / T;           // group inside the warp
+  const int g = warp * GPW + gw;                   // group inside the block
+  const int pair = blockIdx.x * G + g;
+  const bool active = pair < H;
+  const int ya = 2 * pair;
+
+  cpx<SR> v[E];
+  if (active) {
+    const cpx<SR>* S = reinterpret_cast<const cpx<SR>*>(I.S);
+    const cpx<SR>* ra = S + (size_t)ya * H;
+    const cpx<SR>* rb = ra + H;
+    load_pair_rows<P, SR>(v, t, [&](int idx, cpx<SR>& a, cpx<SR>& b) {
+      a = ldc(ra + idx);
+      b = ldc(rb + idx);
+    });
+  } else {
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = mkc<SR>(0, 0);
+  }
+  cpx<SR>* xs = reinterpret_cast<cpx<SR>*>(smraw);
+  const SwizzleLayout<N, sizeof(cpx<SR>)> lay_s{g * N, gw};
+  fft<true, P, WarpSync>(v, t, xs, lay_s, reinterpret_cast<const cpx<SR>*>(I.tw_s));
+
+  const ModelParams mp = I.p;
+  const SR invN = (SR)1 / (SR)N;
+  const WR* phi = reinterpret_cast<const WR*>(I.phi);
+  double sum_c = 0.0, sum_f = 0.0, mn = INFINITY, mx = -INFINITY, bad = 0.0;
+  cpx<WR> wv[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int x = t + T * m;
+    SR fa = 0, fb = 0;
+    if (active) {
+      const SR ca = v[m].x * invN, cb = v[m].y * invN;
+      const SR pa = (SR)__ldg(phi + (size_t)ya * N + x), pb = (SR)__ldg(phi + (size_t)(ya + 1) * N + x);
+      SR ea, eb;
+      bulk<SR>(ca, pa, mp, fa, ea);
+      bulk<SR>(cb, pb, mp, fb, eb);
+      sum_c += (double)ca + (double)cb;
+      sum_f += (double)ea + (double)eb;
+      mn = fmin(mn, fmin((double)ca, (double)cb));
+      mx = fmax(mx, fmax((double)ca, (double)cb));
+      bad += (isfinite((double)ca) ? 0.0 : 1.0) + (isfinite((double)cb) ? 0.0 : 1.0);
+    }
+    wv[m] = mkc<WR>((WR)fa, (WR)fb);
+  }
+  cpx<WR>* xw = reinterpret_cast<cpx<WR>*>(smraw);
+  // the FP32 exchange reuses the group's slice (n elements of the smaller type)
+  const SwizzleLayout<N, sizeof(cpx<WR>)> lay_w{g * N * (int)(sizeof(cpx<SR>) / sizeof(cpx<WR>)), gw};
+  __syncwarp();
+  fft<false, P, WarpSync>(wv, t, xw, lay_w, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  cpx<WR> xa[E / 2], xb[E / 2];
+  split_rows<P, WR>(wv, t, nullptr, RowLayout<N>{0}, xa, xb);
+  if (active) {
+    cpx<WR>* F = reinterpret_cast<cpx<WR>*>(I.F) + (size_t)ya * H;
+#pragma unroll
+    for (int m = 0; m < E / 2; ++m) {
+      F[t + T * m] = xa[m];
+      F[H + t + T * m] = xb[m];
+    }
+  }
+  sum_c = warp_sum(sum_c);
+  mn = warp_min(mn);
+  mx = warp_max(mx);
+  sum_f = warp_sum(sum_f);
+  bad = warp_sum(bad);
+  const int slot = blockIdx.x * NW + warp;
+  if (lane == 0) {
+    double* pp = I.part + (size_t)slot * 5;
+    pp[0] = sum_c;
+    pp[1] = mn;
+    pp[2] = mx;
+    pp[3] = sum_f;
+    pp[4] = bad;
+  }
+  if (!warp_arrive_last(&I.cnt[0], (unsigned)(tiles * NW))) return;
+  const int nslots = tiles * NW;
+  const double a_sum = warp_fold<OpSum>(I.part + 0, nslots, 5, 0.0);
+  const double a_min = warp_fold<OpMin>(I.part + 1, nslots, 5, INFINITY);
+  const double a_max = warp_fold<OpMax>(I.part + 2, nslots, 5, -INFINITY);
+  const double a_f = warp_fold<OpSum>(I.part + 3, nslots, 5, 0.0);
+  const double a_bad = warp_fold<OpSum>(I.part + 4, nslots, 5, 0.0);
+  if (lane == 0) {
+    const int s = step_index(base, s_local);
+    if (I.hist) {
+      const size_t ld = (size_t)I.hist_ld;
+      I.hist[s] = (double)s * I.dt;
+      I.hist[s + 1 * ld] = a_sum / ((double)N * N);
+      I.hist[s + 3 * ld] = a_min;
+      I.hist[s + 4 * ld] = a_max;
+    }
+    I.scal[0] = a_f;
+    if (a_bad > 0.0) {
+      *I.bad_step = s;
+      *I.status = kStatusNonFinite;
+    }
+    I.cnt[0] = 0;
+  }
+}
+
+// =====================================================================================
+template <class P, typename SR, typename WR>
+__global__ void __launch_bounds__(kBlock, 2) k_row_b_w(const InstDev* __restrict__ insts,
+                                                       const int* __restrict__ base, int s_local) {
+  using WG = WarpRowGeom<P>;
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
+  constexpr int tiles = WG::tiles_rows;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const InstDev& I = insts[blockIdx.y];
+  if (!warp_instance_running(I.status)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = lane % T, gw = lane / T;
+  const int g = warp * GPW + gw;
+  const int y = blockIdx.x * G + g;
+  const bool active = y < N;
+  cpx2<WR>* row = reinterpret_cast<cpx2<WR>*>(I.G) + (size_t)(active ? y : 0) * H;
+  cpx<WR> v[E];
+  if (active) {
+    load_pair_rows<P, WR>(v, t, [&](int idx, cpx<WR>& a, cpx<WR>& b) {
+      const cpx2<WR> q = row[idx];
+      a = q.a;
+      b = q.b;
+    });
+  } else {
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = mkc<WR>(0, 0);
+  }
+  cpx<WR>* xw = reinterpret_cast<cpx<WR>*>(smraw);
+  const SwizzleLayout<N, sizeof(cpx<WR>)> lay{g * N, gw};
+  fft<true, P, WarpSync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  const WR* phi = reinterpret_cast<const WR*>(I.phi);
+  const WR M0 = (WR)I.p.mobility;
+  double dsum = 0.0;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    WR M = 0;
+    if (active) {
+      M = mobility_of<WR>(__ldg(phi + (size_t)y * N + t + T * m), M0);
+      dsum += (double)M * ((double)v[m].x * v[m].x + (double)v[m].y * v[m].y);
+    }
+    v[m] = cscale(v[m], M);
+  }
+  fft<false, P, WarpSync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  cpx<WR> xa[E / 2], xb[E / 2];
+  split_rows<P, WR>(v, t, nullptr, RowLayout<N>{0}, xa, xb);
+  __syncwarp();  // every lane of the group has read its inputs before the row is overwritten
+  if (active) {
+#pragma unroll
+    for (int m = 0; m < E / 2; ++m) {
+      cpx2<WR> o;
+      o.a = xa[m];
+      o.b = xb[m];
+      row[t + T * m] = o;
+    }
+  }
+  dsum = warp_sum(dsum);
+  const int slot = blockIdx.x * NW + warp;
+  if (lane == 0) I.part[slot] = dsum;
+  if (!warp_arrive_last(&I.cnt[2], (unsigned)(tiles * NW))) return;
+  const double d = warp_fold<OpSum>(I.part, tiles * NW, 1, 0.0);
+  if (lane == 0) {
+    const int s = step_index(base, s_local);
+    if (I.hist) I.hist[s + 5 * (size_t)I.hist_ld] = d * I.dx * I.dx;
+    I.cnt[2] = 0;
+  }
+}
+
+}  // namespace esc
