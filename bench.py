@@ -287,6 +287,7 @@ def main():
                 "step_frac": value / world * B_ALG_PER_STEP / (peak * 1e9),
                 "phase_ms": {f"{n}x{cnt}": [round(x, 4) for x in msl] for n, cnt, msl in prof}}
     bm_final = [w.cpu().numpy() for w in cm]
+    tuned = [{k: g[k] for k in ("n", "instances", "rows", "cols")} for g in bm.describe()]
     bm.close()
 
     # ---- plain FP64 drop-in on the same workload ----
@@ -354,6 +355,7 @@ def main():
         "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
         "fp64_dropin": fp64, "max_abs_err_vs_fp64": max_err, "clocks": clocks,
         "nonfinite_instances": int(sum(1 for x in bads if x >= 0)),
+        "kernel_families": tuned,
     }
     print(json.dumps(line), flush=True)
     return 0

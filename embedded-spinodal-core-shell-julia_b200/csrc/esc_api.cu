@@ -42,6 +42,15 @@ const esc::KernelSet* find_kernels(int n, int prec) {
 
 thread_local std::string tl_err;
 
+// Smooth synthetic composition used only to time kernel variants.
+__global__ void k_fill_tuning_field(double* c, int n, int count) {
+  const size_t total = (size_t)n * n * count;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % n), y = (int)((i / n) % n);
+    c[i] = 0.5 + 0.01 * sin(6.283185307179586 * (3.0 * x + 5.0 * y) / n);
+  }
+}
+
 // Advances the device-side step counter read by the phase kernels.
 __global__ void k_advance(int* base, int by) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *base += by;
@@ -70,6 +79,9 @@ struct Group {
   bool pipe_rows = false;  // use the persistent TMA-fed row kernels
   bool warp_rows = false;  // use the warp-independent row kernels
   bool pipe_cols = false;  // use the persistent TMA-fed column kernels
+  // autotuner outcome: chosen families and measured ms per launch pair
+  int row_family = -1, col_family = -1;
+  float row_ms[3] = {-1, -1, -1}, col_ms[2] = {-1, -1};
 };
 
 // cuTensorMapEncodeTiled from the driver, looked up once
@@ -376,6 +388,172 @@ void phase_col_b(Group& g, cudaStream_t st) {
     g.ks->col_b(g.d_inst, c, st);
 }
 
+// ---- autotuner -----------------------------------------------------------------
+// For every size group it times each available row family (0 legacy block
+// kernels, 1 persistent TMA pipeline, 2 warp-independent) on row A + row B and
+// each column family (0 legacy, 1 persistent TMA pipeline) on column A + column
+// B, on a smooth synthetic state, and keeps the fastest.  Decisions are cached
+// per process by (n, precision, instances) and, when ESC_TUNE_CACHE names a
+// file, read from / appended to it so that later processes reuse them.
+// ESC_TUNE=0 skips timing and takes the warp rows and legacy columns.
+struct TuneKey {
+  int n, prec, count;
+  bool operator<(const TuneKey& o) const {
+    return n != o.n ? n < o.n : (prec != o.prec ? prec < o.prec : count < o.count);
+  }
+};
+std::map<TuneKey, std::pair<int, int>>& tune_cache() {
+  static std::map<TuneKey, std::pair<int, int>> m;
+  return m;
+}
+void load_tune_file() {
+  static bool loaded = false;
+  if (loaded) return;
+  loaded = true;
+  const char* path = getenv("ESC_TUNE_CACHE");
+  if (!path) return;
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  int n, p, c, r, k;
+  while (fscanf(f, " {\"n\": %d, \"prec\": %d, \"count\": %d, \"rows\": %d, \"cols\": %d}", &n, &p, &c, &r, &k) == 5)
+    tune_cache()[TuneKey{n, p, c}] = {r, k};
+  fclose(f);
+}
+void save_tune(const TuneKey& key, int r, int k) {
+  const char* path = getenv("ESC_TUNE_CACHE");
+  if (!path) return;
+  FILE* f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "{\"n\": %d, \"prec\": %d, \"count\": %d, \"rows\": %d, \"cols\": %d}\n", key.n, key.prec, key.count, r, k);
+  fclose(f);
+}
+bool tuning_enabled() {
+  const char* v = getenv("ESC_TUNE");
+  return !(v && v[0] == '0');
+}
+
+void apply_rows(Group& g, int fam) {
+  g.row_family = fam;
+  g.warp_rows = fam == 2;
+  g.pipe_rows = fam == 1;
+}
+void apply_cols(Group& g, int fam) {
+  g.col_family = fam;
+  g.pipe_cols = fam == 1 && g.pipe_cols;
+}
+
+esc_status autotune(Engine& E) {
+  load_tune_file();
+  cudaStream_t st = E.own;
+  const bool timing = tuning_enabled() && row_family_override() < 0 && pipeline_enabled();
+  bool any = false;
+  for (Group& g : E.groups) {
+    const bool can_pipe_rows = g.pipe_rows, can_warp = g.warp_rows, can_pipe_cols = g.pipe_cols;
+    const TuneKey key{g.n, E.prec, (int)g.members.size()};
+    auto hit = tune_cache().find(key);
+    if (hit != tune_cache().end()) {
+      int r = hit->second.first, k = hit->second.second;
+      if ((r == 2 && !can_warp) || (r == 1 && !can_pipe_rows)) r = 0;
+      apply_rows(g, r);
+      apply_cols(g, (k == 1 && can_pipe_cols) ? 1 : 0);
+      continue;
+    }
+    if (!timing) {
+      if (row_family_override() < 0) apply_rows(g, can_warp ? 2 : (can_pipe_rows ? 1 : 0));
+      else g.row_family = g.warp_rows ? 2 : (g.pipe_rows ? 1 : 0);
+      g.col_family = g.pipe_cols ? 1 : 0;
+      if (row_family_override() < 0 && pipeline_enabled()) apply_cols(g, 0);
+      continue;
+    }
+    any = true;
+  }
+  if (!any) return ESC_OK;
+  // synthetic state for the groups still to be tuned
+  for (Group& g : E.groups) {
+    if (g.row_family >= 0) continue;
+    for (size_t s = 0; s < g.members.size(); ++s) {
+      g.h_inst[s].dt = 0.01;
+      g.h_inst[s].hist = nullptr;
+      g.h_inst[s].hist_ld = 1;
+    }
+    CK(cudaMemcpyAsync(g.d_inst, g.h_inst.data(), g.h_inst.size() * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
+    k_fill_tuning_field<<<1024, 256, 0, st>>>(g.cio, g.n, (int)g.members.size());
+    CK(cudaMemsetAsync(g.status, 0, g.members.size() * sizeof(int), st));
+    CK(cudaMemsetAsync(g.cnt, 0, g.members.size() * 4 * sizeof(unsigned), st));
+    g.ks->init(g.d_inst, (int)g.members.size(), st);
+  }
+  CK(cudaMemsetAsync(E.base, 0, sizeof(int), st));
+  CK(cudaGetLastError());
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int reps = 3;
+  auto time_it = [&](auto&& launch) -> float {
+    launch();  // warm-up
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / reps;
+  };
+  for (Group& g : E.groups) {
+    if (g.row_family >= 0) continue;
+    const bool can_pipe_rows = g.pipe_rows, can_warp = g.warp_rows, can_pipe_cols = g.pipe_cols;
+    // columns first (they leave F/G in place for the rows)
+    float best_c = 1e30f;
+    int best_cf = 0;
+    for (int cf = 0; cf < 2; ++cf) {
+      if (cf == 1 && !can_pipe_cols) continue;
+      g.pipe_cols = cf == 1;
+      const float ms = time_it([&] {
+        phase_col_a(g, E.base, 0, st);
+        phase_col_b(g, st);
+      });
+      g.col_ms[cf] = ms;
+      if (ms < best_c) {
+        best_c = ms;
+        best_cf = cf;
+      }
+    }
+    g.pipe_cols = can_pipe_cols;
+    apply_cols(g, best_cf);
+    float best_r = 1e30f;
+    int best_rf = 0;
+    for (int rf = 0; rf < 3; ++rf) {
+      if ((rf == 1 && !can_pipe_rows) || (rf == 2 && !can_warp)) continue;
+      g.pipe_rows = rf == 1;
+      g.warp_rows = rf == 2;
+      const float ms = time_it([&] {
+        phase_row_a(g, E.base, 0, st);
+        phase_row_b(g, E.base, 0, st);
+      });
+      g.row_ms[rf] = ms;
+      if (ms < best_r) {
+        best_r = ms;
+        best_rf = rf;
+      }
+    }
+    g.pipe_rows = can_pipe_rows;
+    g.warp_rows = can_warp;
+    apply_rows(g, best_rf);
+    const TuneKey key{g.n, E.prec, (int)g.members.size()};
+    tune_cache()[key] = {best_rf, best_cf};
+    save_tune(key, best_rf, best_cf);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  // tuning may have flagged nothing, but leave a clean slate for the first run
+  for (Group& g : E.groups) {
+    CK(cudaMemset(g.status, 0, g.members.size() * sizeof(int)));
+    CK(cudaMemset(g.cnt, 0, g.members.size() * 4 * sizeof(unsigned)));
+  }
+  return ESC_OK;
+}
+
 void launch_step(Engine& E, int s_local, cudaStream_t st) {
   for (Group& g : E.groups) {
     phase_row_a(g, E.base, s_local, st);
@@ -574,7 +752,8 @@ esc_status esc_create(esc_ctx** out, int n, double dx, const double* phi, const 
     return ESC_ENOMEM;
   }
   const double* phis[1] = {phi};
-  const esc_status s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
+  esc_status s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
+  if (s == ESC_OK) s = autotune(c->e);
   if (s != ESC_OK) {
     tl_err = c->e.err;
     c->e.release();
@@ -639,7 +818,8 @@ esc_status esc_batch_create(esc_batch** out, int count, const int* n, const doub
     tl_err = "host allocation failed";
     return ESC_ENOMEM;
   }
-  const esc_status s = engine_create(b->e, count, n, dx, phi, p, (int)prec);
+  esc_status s = engine_create(b->e, count, n, dx, phi, p, (int)prec);
+  if (s == ESC_OK) s = autotune(b->e);
   if (s != ESC_OK) {
     tl_err = b->e.err;
     b->e.release();
@@ -737,6 +917,30 @@ esc_status esc_batch_profile_phases(esc_batch* b, int steps, int* n_groups, int*
     for (int k = 0; k < 4; ++k) ms[4 * gi + k] = acc[4 * gi + k] / steps;
   }
   return ESC_OK;
+}
+
+int esc_batch_describe(const esc_batch* b, char* buf, int buflen) {
+  if (!b) return -1;
+  std::string out = "[";
+  static const char* rows[3] = {"block", "tma-pipeline", "warp"};
+  static const char* cols[2] = {"block", "tma-pipeline"};
+  for (size_t i = 0; i < b->e.groups.size(); ++i) {
+    const Group& g = b->e.groups[i];
+    char tmp[512];
+    snprintf(tmp, sizeof tmp,
+             "%s{\"n\": %d, \"instances\": %zu, \"rows\": \"%s\", \"cols\": \"%s\", \"row_ms\": [%.4f, %.4f, %.4f], "
+             "\"col_ms\": [%.4f, %.4f], \"E\": %d}",
+             i ? ", " : "", g.n, g.members.size(), g.row_family >= 0 ? rows[g.row_family] : "?",
+             g.col_family >= 0 ? cols[g.col_family] : "?", g.row_ms[0], g.row_ms[1], g.row_ms[2], g.col_ms[0],
+             g.col_ms[1], g.ks->E);
+    out += tmp;
+  }
+  out += "]";
+  if (buf && buflen > 0) {
+    strncpy(buf, out.c_str(), (size_t)buflen - 1);
+    buf[buflen - 1] = 0;
+  }
+  return (int)out.size() + 1;
 }
 
 esc_status esc_batch_set_stream(esc_batch* b, void* stream) {

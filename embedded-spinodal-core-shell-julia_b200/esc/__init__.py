@@ -109,6 +109,7 @@ _SIGNATURES = [
     ("esc_batch_profile_phases", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                                 _dp]),
+    ("esc_batch_describe", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int]),
     ("esc_batch_last_error", ctypes.c_char_p, [_vp]),
     ("esc_batch_destroy", None, [_vp]),
 ]
@@ -293,6 +294,15 @@ class Batch:
         if st != ESC_OK:
             _raise(st, self._err())
         return [(int(gn[i]), int(gc[i]), [float(x) for x in ms[4 * i:4 * i + 4]]) for i in range(ng.value)]
+
+    def describe(self):
+        """The autotuner's choice of kernel families per size group (list of dicts)."""
+        import json
+        lib = load_library()
+        need = lib.esc_batch_describe(self._h, None, 0)
+        buf = ctypes.create_string_buffer(max(need, 1))
+        lib.esc_batch_describe(self._h, buf, len(buf))
+        return json.loads(buf.value.decode())
 
     def set_stream(self, stream_ptr: int) -> None:
         st = load_library().esc_batch_set_stream(self._h, _vp(stream_ptr) if stream_ptr else None)

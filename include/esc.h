@@ -120,6 +120,12 @@ esc_status esc_batch_set_stream(esc_batch *b, void *stream);
  * the arrays NULL to size them.  The history buffer row 0 is overwritten. */
 esc_status esc_batch_profile_phases(esc_batch *b, int steps, int *n_groups, int *group_n, int *group_count,
                                     double *ms);
+/* Writes a JSON description of the kernel families the autotuner chose for each
+ * size group (with the per-family timings it measured) into buf; returns the
+ * length needed including the terminating zero.  The tuner runs once per
+ * (n, precision, instance count) at creation on a synthetic state; ESC_TUNE=0
+ * disables it and ESC_TUNE_CACHE=<file> persists its decisions. */
+int esc_batch_describe(const esc_batch *b, char *buf, int buflen);
 const char *esc_batch_last_error(const esc_batch *b);
 
 /* Allocation-free single-particle run.  No counterpart in the reference: it
