@@ -148,6 +148,24 @@ struct Engine {
   cudaGraphExec_t gexec = nullptr;
   std::vector<void*> allocs;
   std::string err;
+  // adjoint resources (allocated on first use; single-instance contexts)
+  struct Adj {
+    bool ready = false;
+    int ckpt_cap = 0, seg_cap = 0;
+    const esc::KernelSet* ks64 = nullptr;
+    double *phi64 = nullptr, *target = nullptr, *part = nullptr, *scal = nullptr, *hist = nullptr,
+           *acc = nullptr, *cout = nullptr;
+    double2 *F64 = nullptr, *Lam = nullptr, *Xg = nullptr, *ckpt = nullptr, *seg = nullptr;
+    esc::cpx2<double>* G64 = nullptr;
+    void* tw64 = nullptr;
+    unsigned *cnt = nullptr, *acnt = nullptr;
+    int *status = nullptr, *zero = nullptr;
+    long long* bad = nullptr;
+    esc::InstDev* d_seed = nullptr;  // FP64 shadow instance with a 1-row history
+    esc::InstDev* d_bwd = nullptr;   // FP64 shadow instance without history
+    esc::InstDev* d_out = nullptr;   // final transform of the adjoint
+    esc::AdjDev* d_adj = nullptr;    // one per step of a segment
+  } adj;
 
   esc_status fail(esc_status s, const std::string& msg) {
     err = msg;
@@ -710,6 +728,204 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
 
 }  // namespace
 
+// ---- adjoint driver -----------------------------------------------------------------
+// L = 1/2 sum (c_T - c_target)^2 + lamF F[c_T]; gradients w.r.t. c0 and
+// theta = (P, chi, kappa, M0).  Forward pass in the context's precision with a
+// checkpoint every `K` steps; backward pass recomputes each segment (storing its
+// states) and applies the FP64 adjoint step (esc_adjoint.cuh) from the last step
+// to the first.
+esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, const double* c_target, double lamF,
+                          int K, double* dL_dc0, double* dL_dparams, double* Lout) {
+  if (E.count != 1) return E.fail(ESC_EINVAL, "esc_adjoint needs a single-particle context");
+  if (steps < 1 || !c0 || !c_target) return E.fail(ESC_EINVAL, "bad adjoint arguments");
+  if (!std::isfinite(dt) || !std::isfinite(lamF)) return E.fail(ESC_EINVAL, "dt and lambda_F must be finite");
+  if (K < 1) K = (int)std::ceil(std::sqrt((double)steps));
+  if (K > steps) K = steps;
+  DeviceGuard dg(E.device);
+  Group& g = E.groups[0];
+  const int n = g.n, H = n / 2;
+  const size_t nn = (size_t)n * n;
+  auto& A = E.adj;
+  cudaStream_t st = E.stream;
+  const int nck = (steps + K - 1) / K;
+  if (!A.ready) {
+    A.ks64 = find_kernels(n, ESC_FP64);
+    if (!A.ks64 || !A.ks64->adj_col1) return E.fail(ESC_EINVAL, "no adjoint kernels for this size");
+    CK(A.ks64->prepare());
+    CK(A.ks64->prepare_adj());
+    TRY(E.alloc(&A.phi64, nn * 8, "adjoint phi"));
+    TRY(E.alloc(&A.target, nn * 8, "adjoint target"));
+    TRY(E.alloc(&A.cout, nn * 8, "adjoint output"));
+    TRY(E.alloc(&A.F64, (size_t)H * n * 16, "adjoint F"));
+    TRY(E.alloc(&A.Lam, (size_t)H * n * 16, "adjoint state"));
+    TRY(E.alloc(&A.Xg, (size_t)H * n * 16, "adjoint Xg"));
+    TRY(E.alloc(&A.G64, (size_t)H * n * 32, "adjoint G"));
+    TRY(E.alloc(&A.tw64, (size_t)n * 16, "adjoint twiddles"));
+    TRY(E.alloc(&A.part, (size_t)(A.ks64->part_len + 8 * 4096) * 8, "adjoint partials"));
+    TRY(E.alloc(&A.scal, 64, "adjoint scalars"));
+    TRY(E.alloc(&A.hist, 6 * 8, "adjoint history row"));
+    TRY(E.alloc(&A.acc, 8 * 8, "adjoint accumulators"));
+    TRY(E.alloc(&A.cnt, 4 * 4, "adjoint counters"));
+    TRY(E.alloc(&A.acnt, 4 * 4, "adjoint counters"));
+    TRY(E.alloc(&A.status, 4, "adjoint status"));
+    TRY(E.alloc(&A.zero, 4, "zero"));
+    TRY(E.alloc(&A.bad, 8, "adjoint bad step"));
+    TRY(E.alloc(&A.d_seed, sizeof(esc::InstDev), "adjoint descriptor"));
+    TRY(E.alloc(&A.d_bwd, sizeof(esc::InstDev), "adjoint descriptor"));
+    TRY(E.alloc(&A.d_out, sizeof(esc::InstDev), "adjoint descriptor"));
+    // FP64 particle field and twiddles
+    if (g.ks->wr_bytes == 8) {
+      CK(cudaMemcpy(A.phi64, g.phi, nn * 8, cudaMemcpyDeviceToDevice));
+    } else {
+      std::vector<float> pf(nn);
+      std::vector<double> pd(nn);
+      CK(cudaMemcpy(pf.data(), g.phi, nn * 4, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < nn; ++k) pd[k] = (double)pf[k];
+      CK(cudaMemcpy(A.phi64, pd.data(), nn * 8, cudaMemcpyHostToDevice));
+    }
+    if (g.ks->sr_bytes == 8) CK(cudaMemcpy(A.tw64, g.tw_s, (size_t)n * 16, cudaMemcpyDeviceToDevice));
+    CK(cudaMemset(A.zero, 0, 4));
+    A.ready = true;
+  }
+  if (nck > A.ckpt_cap) {
+    TRY(E.alloc(&A.ckpt, (size_t)nck * H * n * 16, "adjoint checkpoints"));
+    A.ckpt_cap = nck;
+  }
+  if (K + 1 > A.seg_cap) {
+    TRY(E.alloc(&A.seg, (size_t)(K + 1) * H * n * 16, "adjoint segment"));
+    TRY(E.alloc(&A.d_adj, (size_t)K * sizeof(esc::AdjDev), "adjoint step descriptors"));
+    A.seg_cap = K + 1;
+  }
+  const size_t sbytes = (size_t)H * n * 16;
+  double2* S = static_cast<double2*>(g.S);
+  // ---- forward pass with checkpoints ----
+  esc::InstDev& d = g.h_inst[0];
+  d.dt = dt;
+  d.hist = nullptr;
+  d.hist_ld = 1;
+  d.cio = g.cio;
+  CK(cudaMemcpyAsync(g.d_inst, &d, sizeof d, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(g.cio, c0, nn * 8, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(A.target, c_target, nn * 8, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(g.status, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(g.cnt, 0, 4 * sizeof(unsigned), st));
+  CK(cudaMemsetAsync(E.base, 0, sizeof(int), st));
+  g.ks->init(g.d_inst, 1, st);
+  for (int s = 0; s < steps; ++s) {
+    if (s % K == 0) CK(cudaMemcpyAsync(A.ckpt + (size_t)(s / K) * H * n, S, sbytes, cudaMemcpyDeviceToDevice, st));
+    launch_step(E, 0, st);
+  }
+  CK(cudaGetLastError());
+  // ---- seed: energy, mu and lam_T at the final field ----
+  const esc::KernelSet* k64 = A.ks64;
+  esc::InstDev sd;
+  memset(&sd, 0, sizeof sd);
+  sd.n = n;
+  sd.hist_ld = 1;
+  sd.dx = g.h_inst[0].dx;
+  sd.dt = dt;
+  sd.p = g.h_inst[0].p;
+  sd.S = S;
+  sd.F = A.F64;
+  sd.G = A.G64;
+  sd.phi = A.phi64;
+  sd.hist = A.hist;
+  sd.part = A.part;
+  sd.cnt = A.cnt;
+  sd.scal = A.scal;
+  sd.status = A.status;
+  sd.bad_step = A.bad;
+  sd.tw_s = A.tw64;
+  sd.tw_w = A.tw64;
+  sd.cio = A.cout;
+  esc::InstDev bd = sd;
+  bd.hist = nullptr;
+  esc::InstDev od = sd;
+  od.S = A.Lam;
+  od.hist = nullptr;
+  CK(cudaMemcpyAsync(A.d_seed, &sd, sizeof sd, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(A.d_bwd, &bd, sizeof bd, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(A.d_out, &od, sizeof od, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(A.cnt, 0, 16, st));
+  CK(cudaMemsetAsync(A.acnt, 0, 16, st));
+  CK(cudaMemsetAsync(A.status, 0, 4, st));
+  CK(cudaMemsetAsync(A.acc, 0, 64, st));
+  k64->row_a(A.d_seed, 1, A.zero, 0, st);
+  k64->col_a(A.d_seed, 1, A.zero, 0, st);
+  esc::AdjDev ad;
+  memset(&ad, 0, sizeof ad);
+  ad.n = n;
+  ad.dx = sd.dx;
+  ad.dt = dt;
+  ad.lamF = lamF;
+  ad.p = sd.p;
+  ad.S0 = S;
+  ad.S1 = S;
+  ad.Lam = A.Lam;
+  ad.Xg = A.Xg;
+  ad.F = A.F64;
+  ad.G = A.G64;
+  ad.phi = A.phi64;
+  ad.target = A.target;
+  ad.tw = A.tw64;
+  ad.part = A.part;
+  ad.cnt = A.acnt;
+  ad.acc = A.acc;
+  CK(cudaMemcpyAsync(A.d_adj, &ad, sizeof ad, cudaMemcpyHostToDevice, st));
+  k64->adj_mu_col(A.d_adj, 1, st);
+  k64->adj_seed_row(A.d_adj, 1, st);
+  double hist_row[6], scal0 = 0.0;
+  CK(cudaMemcpyAsync(hist_row, A.hist, sizeof hist_row, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&scal0, A.scal, sizeof scal0, cudaMemcpyDeviceToHost, st));
+  CK(cudaGetLastError());
+  // ---- backward over segments ----
+  std::vector<esc::AdjDev> steps_desc((size_t)K);
+  for (int seg = nck - 1; seg >= 0; --seg) {
+    const int s0 = seg * K, s1 = std::min(steps, s0 + K), len = s1 - s0;
+    const double2* ck = A.ckpt + (size_t)seg * H * n;
+    CK(cudaMemcpyAsync(A.seg, ck, sbytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(S, ck, sbytes, cudaMemcpyDeviceToDevice, st));
+    for (int j = 1; j <= len; ++j) {
+      launch_step(E, 0, st);
+      CK(cudaMemcpyAsync(A.seg + (size_t)j * H * n, S, sbytes, cudaMemcpyDeviceToDevice, st));
+    }
+    for (int j = 0; j < len; ++j) {
+      steps_desc[j] = ad;
+      steps_desc[j].S0 = A.seg + (size_t)j * H * n;
+      steps_desc[j].S1 = A.seg + (size_t)(j + 1) * H * n;
+    }
+    CK(cudaMemcpyAsync(A.d_adj, steps_desc.data(), (size_t)len * sizeof(esc::AdjDev), cudaMemcpyHostToDevice, st));
+    for (int j = len - 1; j >= 0; --j) {
+      k64->adj_col1(A.d_adj + j, 1, st);
+      k64->row_b(A.d_bwd, 1, A.zero, 0, st);
+      k64->adj_col2(A.d_adj + j, 1, st);
+      k64->adj_row2(A.d_adj + j, 1, st);
+    }
+    // the descriptors of this segment must not be overwritten before its kernels ran
+    CK(cudaStreamSynchronize(st));
+  }
+  CK(cudaGetLastError());
+  k64->fin(A.d_out, 1, st);
+  double acc[8];
+  CK(cudaMemcpyAsync(acc, A.acc, sizeof acc, cudaMemcpyDeviceToHost, st));
+  if (dL_dc0) CK(cudaMemcpyAsync(dL_dc0, A.cout, nn * 8, cudaMemcpyDeviceToHost, st));
+  int fstatus = 0;
+  CK(cudaMemcpyAsync(&fstatus, g.status, sizeof fstatus, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (fstatus) return E.fail(ESC_ENONFINITE, "Non-finite composition during the adjoint's forward pass");
+  const double dx2 = sd.dx * sd.dx;
+  const double E_T = hist_row[2];
+  const esc::ModelParams& p = sd.p;
+  if (dL_dparams) {
+    dL_dparams[0] = acc[0] + lamF * acc[5] * dx2;
+    dL_dparams[1] = acc[1] + lamF * (-p.P * acc[6] * dx2);
+    dL_dparams[2] = acc[2] + lamF * ((E_T - scal0 * dx2) / p.kappa);
+    dL_dparams[3] = acc[3];
+  }
+  if (Lout) *Lout = acc[4] + lamF * E_T;
+  return ESC_OK;
+}
+
 // Lets other translation units of the library report through esc_last_error(NULL).
 void esc_set_thread_error(const char* msg) { tl_err = msg ? msg : ""; }
 
@@ -917,6 +1133,15 @@ esc_status esc_batch_profile_phases(esc_batch* b, int steps, int* n_groups, int*
     for (int k = 0; k < 4; ++k) ms[4 * gi + k] = acc[4 * gi + k] / steps;
   }
   return ESC_OK;
+}
+
+esc_status esc_adjoint(esc_ctx* ctx, const double* c0, int steps, double dt, const double* c_target,
+                       double lambda_F, int ckpt_every, double* dL_dc0, double* dL_dparams, double* L) {
+  if (!ctx) {
+    tl_err = "null context";
+    return ESC_EINVAL;
+  }
+  return engine_adjoint(ctx->e, c0, steps, dt, c_target, lambda_F, ckpt_every, dL_dc0, dL_dparams, L);
 }
 
 int esc_batch_describe(const esc_batch* b, char* buf, int buflen) {

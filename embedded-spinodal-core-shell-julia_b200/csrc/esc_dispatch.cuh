@@ -1,7 +1,9 @@
 // Per-size kernel sets: launch wrappers and launch geometry for one grid size n
 // and one precision mode.  Each esc_size_<n>.cu instantiates the two modes.
 #pragma once
+#include <type_traits>
 #include "esc_warp.cuh"
+#include "esc_adjoint.cuh"
 
 namespace esc {
 
@@ -33,6 +35,13 @@ struct KernelSet {
   void (*row_a_w)(const InstDev*, int, const int*, int, cudaStream_t);
   void (*row_b_w)(const InstDev*, int, const int*, int, cudaStream_t);
   cudaError_t (*prepare_warp)();
+  // adjoint step kernels (FP64 kernel sets only; null in the mixed sets)
+  cudaError_t (*prepare_adj)();
+  void (*adj_col1)(const AdjDev*, int, cudaStream_t);
+  void (*adj_col2)(const AdjDev*, int, cudaStream_t);
+  void (*adj_row2)(const AdjDev*, int, cudaStream_t);
+  void (*adj_mu_col)(const AdjDev*, int, cudaStream_t);
+  void (*adj_seed_row)(const AdjDev*, int, cudaStream_t);
 };
 
 // FP64 plans keep E <= 16 so that two register arrays of double2 fit.
@@ -208,6 +217,36 @@ struct KS {
     if constexpr (warp_ok)
       k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kBlock, warp_smem(), st>>>(d, base, s);
   }
+  // ---- adjoint (FP64) ----
+  static constexpr bool adj_ok = std::is_same<SR, double>::value && std::is_same<WR, double>::value;
+  static cudaError_t prepare_adj() {
+    if constexpr (adj_ok) {
+      const int bytes = (int)smem();
+      cudaError_t e;
+      if ((e = cudaFuncSetAttribute(k_adj_col1<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+      if ((e = cudaFuncSetAttribute(k_adj_col2<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+      if ((e = cudaFuncSetAttribute(k_adj_row2<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+      if ((e = cudaFuncSetAttribute(k_adj_mu_col<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+      if ((e = cudaFuncSetAttribute(k_adj_seed_row<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
+        return e;
+    }
+    return cudaSuccess;
+  }
+  static void adj_col1(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_col1<P><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(a);
+  }
+  static void adj_col2(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_col2<P><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(a);
+  }
+  static void adj_row2(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_row2<P><<<dim3(tiles_pairs, count), kBlock, smem(), st>>>(a);
+  }
+  static void adj_mu_col(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_mu_col<P><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(a);
+  }
+  static void adj_seed_row(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_seed_row<P><<<dim3(tiles_pairs, count), kBlock, smem(), st>>>(a);
+  }
   static KernelSet make(int prec) {
     KernelSet k;
     k.n = N;
@@ -248,6 +287,12 @@ struct KS {
     k.row_a_w = &row_a_w;
     k.row_b_w = &row_b_w;
     k.prepare_warp = &prepare_warp;
+    k.prepare_adj = &prepare_adj;
+    k.adj_col1 = adj_ok ? &adj_col1 : nullptr;
+    k.adj_col2 = adj_ok ? &adj_col2 : nullptr;
+    k.adj_row2 = adj_ok ? &adj_row2 : nullptr;
+    k.adj_mu_col = adj_ok ? &adj_mu_col : nullptr;
+    k.adj_seed_row = adj_ok ? &adj_seed_row : nullptr;
     return k;
   }
 };

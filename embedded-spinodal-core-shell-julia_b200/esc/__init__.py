@@ -99,6 +99,8 @@ _SIGNATURES = [
     ("esc_set_stream", ctypes.c_int, [_vp, _vp]),
     ("esc_last_error", ctypes.c_char_p, [_vp]),
     ("esc_destroy", None, [_vp]),
+    ("esc_adjoint", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_int,
+                                   _dp, _dp, _dp]),
     ("esc_batch_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                         _dp, ctypes.POINTER(_dp), ctypes.POINTER(_CParams), ctypes.c_int]),
     ("esc_batch_run", ctypes.c_int, [_vp, ctypes.POINTER(_dp), ctypes.c_int, ctypes.c_double,
@@ -192,6 +194,20 @@ class Context:
         if st != ESC_OK:
             _raise(st, self._err(), bad.value)
         return c, (hist.T.copy() if hist is not None else None)
+
+    def adjoint(self, c0, c_target, dt: float = 0.01, steps: int = 100, lambda_F: float = 1e-3,
+                ckpt_every: int = 0):
+        """(L, dL/dc0, dL/d(P, chi, kappa, M0)) for L = 1/2 |c_T - c_target|^2 + lambda_F F[c_T]."""
+        c0 = _field(c0, self.n, "c0")
+        ct = _field(c_target, self.n, "c_target")
+        g = np.zeros((self.n, self.n))
+        dp = np.zeros(4)
+        L = ctypes.c_double(0.0)
+        st = load_library().esc_adjoint(self._h, _ptr(c0), int(steps), float(dt), _ptr(ct), float(lambda_F),
+                                        int(ckpt_every), _ptr(g), _ptr(dp), ctypes.byref(L))
+        if st != ESC_OK:
+            _raise(st, self._err())
+        return L.value, g, dp
 
     def run_device(self, c_ptr: int, steps: int, dt: float, hist_ptr: int = 0) -> None:
         """esc_run_device on caller-owned device buffers (raw addresses)."""

@@ -90,6 +90,17 @@ const char *esc_last_error(const esc_ctx *ctx);
 
 void esc_destroy(esc_ctx *ctx);
 
+/* Gradient of L = 1/2 sum_x (c_T - c_target)^2 + lambda_F * F[c_T] (F the energy
+ * of core_shell.jl:78-82, c_T after `steps` steps from c0) with respect to c0
+ * (dL_dc0, n*n) and to theta = (P, chi, kappa, M0) (dL_dparams, 4 values), by a
+ * hand-written FP64 adjoint of the stabilised update with checkpoint-and-
+ * recompute every ckpt_every steps (<= 0: ceil(sqrt(steps))).  The forward and
+ * recomputed passes run in the context's precision.  Any output may be NULL.
+ * No counterpart in the reference (which has no gradients); it serves parameter
+ * calibration. */
+esc_status esc_adjoint(esc_ctx *ctx, const double *c0, int steps, double dt, const double *c_target,
+                       double lambda_F, int ckpt_every, double *dL_dc0, double *dL_dparams, double *L);
+
 /* Batched ensemble: `count` independent particles with their own grid size n[i],
  * spacing dx[i], particle phi[i] (n[i]^2) and constants p[i], advanced together
  * (same dt, same step count).  Grid sizes may differ. */

@@ -1,0 +1,81 @@
+"""GPU adjoint (esc_adjoint through the C ABI) against the CPU oracle.
+
+Checks, on small grids and in FP64: the loss, dL/dc0 and dL/d(P, chi, kappa, M0)
+against the oracle's reverse mode; the directional derivative against the
+oracle's forward (dual-number) mode; parameter gradients against central
+finite differences (h = 1e-4, FP64) of the GPU forward itself.
+"""
+import numpy as np
+import pytest
+
+import esc
+from oracle import adjoint_oracle as adj
+from oracle import core_shell_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(n, steps, seed=3):
+    p = orc.Parameters()
+    c0, phi = orc.initial_fields(n, radius=n / 4, width=2.0, seed=seed)
+    pt = adj._with(p, P=p.P * 1.1, chi=p.chi * 0.9)           # target: perturbed (P, chi)
+    ct = adj.forward_states(c0, phi, steps, 0.01, pt)[-1]
+    return p, c0, phi, ct
+
+
+def _ep(p):
+    return esc.Parameters(A=p.A, B=p.B, chi=p.chi, P=p.P, ca=p.ca, cb=p.cb, cc=p.cc, kappa=p.kappa,
+                          mobility=p.mobility, Q=p.Q)
+
+
+@pytest.mark.parametrize("n,steps,K", [(32, 30, 7), (64, 45, 0), (48, 20, 20)])
+def test_adjoint_matches_oracle(n, steps, K):
+    p, c0, phi, ct = _case(n, steps)
+    lamF = 1e-3
+    Lo, go, tho = adj.gradient(c0, phi, steps, 0.01, ct, lamF, p)
+    with esc.Context(phi, p=_ep(p)) as ctx:
+        L, g, th = ctx.adjoint(c0, ct, dt=0.01, steps=steps, lambda_F=lamF, ckpt_every=K)
+    assert abs(L - Lo) <= 1e-12 * abs(Lo)
+    assert np.max(np.abs(g - go)) <= 1e-10 * np.max(np.abs(go))
+    assert np.max(np.abs(th - tho) / np.maximum(np.abs(tho), 1e-30)) <= 1e-9, (th, tho)
+
+
+def test_adjoint_directional_derivative_vs_dual_numbers():
+    n, steps = 64, 40
+    p, c0, phi, ct = _case(n, steps, seed=8)
+    rng = np.random.default_rng(8)
+    v = rng.standard_normal(c0.shape)
+    th_dir = rng.standard_normal(4)
+    jv = adj.jvp(c0, phi, steps, 0.01, ct, 1e-3, p, v, th_dir)
+    with esc.Context(phi, p=_ep(p)) as ctx:
+        _, g, th = ctx.adjoint(c0, ct, dt=0.01, steps=steps, lambda_F=1e-3)
+    ad = float(np.sum(g * v) + np.dot(th, th_dir))
+    assert abs(ad - jv) <= 1e-9 * abs(jv)
+
+
+def test_adjoint_parameters_vs_central_differences():
+    n, steps, lamF, h = 64, 40, 1e-3, 1e-4
+    p, c0, phi, ct = _case(n, steps, seed=5)
+
+    def gpu_loss(pp):
+        c, hist = esc.run_simulation(c0, phi, dt=0.01, steps=steps, p=_ep(pp))
+        return 0.5 * float(np.sum((c - ct) ** 2)) + lamF * hist[-1, 2]
+
+    with esc.Context(phi, p=_ep(p)) as ctx:
+        _, _, th = ctx.adjoint(c0, ct, dt=0.01, steps=steps, lambda_F=lamF)
+    tol = {0: 1e-6, 1: 1e-6, 2: 1e-4, 3: 1e-5}
+    for k in range(4):
+        fd = (gpu_loss(adj.perturbed(p, k, h)) - gpu_loss(adj.perturbed(p, k, -h))) / (2 * h)
+        assert abs(fd - th[k]) <= tol[k] * max(abs(fd), 1e-12), (adj.THETA[k], fd, th[k])
+
+
+def test_adjoint_mixed_precision_close_to_fp64():
+    n, steps = 64, 40
+    p, c0, phi, ct = _case(n, steps)
+    with esc.Context(phi, p=_ep(p)) as c64:
+        L64, g64, th64 = c64.adjoint(c0, ct, dt=0.01, steps=steps)
+    with esc.Context(phi, p=_ep(p), precision="mixed") as c32:
+        L32, g32, th32 = c32.adjoint(c0, ct, dt=0.01, steps=steps)
+    assert abs(L32 - L64) <= 1e-6 * abs(L64)
+    assert np.max(np.abs(g32 - g64)) <= 1e-4 * np.max(np.abs(g64))
+    assert np.max(np.abs(th32 - th64) / np.abs(th64)) <= 1e-3
