@@ -11,6 +11,9 @@ is one time step of every particle (history row + stabilised update).
   e2e     the same through esc_batch_run with pinned host buffers: the H2D copy
           of c0 and the D2H copy of c and of the history are inside the timing
   fp64    the plain FP64 drop-in on the same workload (the 5x target's denominator)
+  adjoint gradient of 1/2|c_T - c_target|^2 + 1e-3 F[c_T] w.r.t. c0 and (P, chi, kappa, M0)
+          through 2000 mixed-precision steps at 256^2 and 512^2 (checkpoints every 45):
+          the reverse sweep (recompute + adjoint) per step over the forward step
 
 The working set (1.7 GB mixed, 2.6 GB FP64) is far larger than the 126 MB L2,
 so no flush is needed between steps.  Under torchrun every rank runs its own
@@ -197,6 +200,7 @@ def main():
     ap.add_argument("--count", type=int, default=COUNT)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -329,6 +333,32 @@ def main():
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
            "note": "one esc_batch_run call of K steps: c0 H2D once, c and history D2H once (per-step share shown)"}
 
+    # ---- adjoint / forward time (calibration workload: 256^2 and 512^2, 2000 steps) ----
+    adjoint = None
+    if not args.no_adjoint:
+        from esc import fields
+        adjoint = []
+        for n in (256, 512):
+            phi = fields.particle_disc(n, radius=0.35 * n, width=2.0)
+            c0 = fields.interior_noise(phi, 1)
+            base_p = esc.Parameters()
+            pt = esc.Parameters(P=base_p.P * 1.1, chi=base_p.chi * 0.9)
+            ct, _ = esc.run_simulation(c0, phi, dt=DT, steps=2000, p=pt, precision="mixed")
+            with esc.Context(phi, precision="mixed") as ctx:
+                ctx.run(c0, dt=DT, steps=20, with_history=False)
+                ctx.adjoint(c0, ct, dt=DT, steps=20, lambda_F=1e-3, ckpt_every=5)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                ctx.run(c0, dt=DT, steps=2000, with_history=False)
+                tf = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                L, g, th = ctx.adjoint(c0, ct, dt=DT, steps=2000, lambda_F=1e-3, ckpt_every=45)
+                ta = time.perf_counter() - t0
+            adjoint.append({"n": n, "steps": 2000, "ckpt_every": 45, "forward_s": tf, "adjoint_call_s": ta,
+                            "reverse_step_over_forward_step": (ta - tf) / tf,
+                            "adjoint_call_over_forward": ta / tf,
+                            "dL_dtheta": [float(x) for x in th]})
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         idx = sample_subset(ns)
@@ -354,6 +384,7 @@ def main():
                    "global_batch": args.count * world, "l2": "working set 1.7 GB >> 126 MB L2; no flush"},
         "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
         "fp64_dropin": fp64, "max_abs_err_vs_fp64": max_err, "clocks": clocks,
+        "adjoint": adjoint,
         "nonfinite_instances": int(sum(1 for x in bads if x >= 0)),
         "kernel_families": tuned,
     }

@@ -81,7 +81,7 @@ struct Group {
   bool pipe_cols = false;  // use the persistent TMA-fed column kernels
   // autotuner outcome: chosen families and measured ms per launch pair
   int row_family = -1, col_family = -1;
-  float row_ms[3] = {-1, -1, -1}, col_ms[2] = {-1, -1};
+  float row_ms[3] = {-1, -1, -1}, col_ms[3] = {-1, -1, -1};
 };
 
 // cuTensorMapEncodeTiled from the driver, looked up once
@@ -146,6 +146,9 @@ struct Engine {
   double* hist = nullptr;
   size_t hist_cap = 0;  // doubles
   cudaGraphExec_t gexec = nullptr;
+  std::vector<cudaStream_t> side;    // per-group capture streams
+  std::vector<cudaEvent_t> side_ev;  // per-group join events
+  cudaEvent_t fork_ev = nullptr;
   std::vector<void*> allocs;
   std::string err;
   // adjoint resources (allocated on first use; single-instance contexts)
@@ -191,6 +194,12 @@ struct Engine {
   void release() {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
+    for (cudaStream_t s : side) cudaStreamDestroy(s);
+    side.clear();
+    for (cudaEvent_t e : side_ev) cudaEventDestroy(e);
+    side_ev.clear();
+    if (fork_ev) cudaEventDestroy(fork_ev);
+    fork_ev = nullptr;
     for (void* q : allocs) cudaFree(q);
     allocs.clear();
     if (own) cudaStreamDestroy(own);
@@ -384,7 +393,9 @@ void phase_row_a(Group& g, const int* base, int s_local, cudaStream_t st) {
 }
 void phase_col_a(Group& g, const int* base, int s_local, cudaStream_t st) {
   const int c = (int)g.members.size();
-  if (g.pipe_cols)
+  if (g.col_family == 2)
+    g.ks->col_a_alt(g.d_inst, c, base, s_local, st);
+  else if (g.pipe_cols)
     g.ks->col_a_p(g.d_inst, c, base, s_local, st, &g.maps);
   else
     g.ks->col_a(g.d_inst, c, base, s_local, st);
@@ -400,7 +411,9 @@ void phase_row_b(Group& g, const int* base, int s_local, cudaStream_t st) {
 }
 void phase_col_b(Group& g, cudaStream_t st) {
   const int c = (int)g.members.size();
-  if (g.pipe_cols)
+  if (g.col_family == 2)
+    g.ks->col_b_alt(g.d_inst, c, st);
+  else if (g.pipe_cols)
     g.ks->col_b_p(g.d_inst, c, st, &g.maps);
   else
     g.ks->col_b(g.d_inst, c, st);
@@ -459,6 +472,7 @@ void apply_cols(Group& g, int fam) {
   g.col_family = fam;
   g.pipe_cols = fam == 1 && g.pipe_cols;
 }
+// column family 2 (alternative plan) needs no capability beyond the kernel set
 
 esc_status autotune(Engine& E) {
   load_tune_file();
@@ -473,7 +487,7 @@ esc_status autotune(Engine& E) {
       int r = hit->second.first, k = hit->second.second;
       if ((r == 2 && !can_warp) || (r == 1 && !can_pipe_rows)) r = 0;
       apply_rows(g, r);
-      apply_cols(g, (k == 1 && can_pipe_cols) ? 1 : 0);
+      apply_cols(g, (k == 1 && !can_pipe_cols) ? 0 : k);
       continue;
     }
     if (!timing) {
@@ -522,9 +536,11 @@ esc_status autotune(Engine& E) {
     // columns first (they leave F/G in place for the rows)
     float best_c = 1e30f;
     int best_cf = 0;
-    for (int cf = 0; cf < 2; ++cf) {
+    for (int cf = 0; cf < 3; ++cf) {
       if (cf == 1 && !can_pipe_cols) continue;
+      if (cf == 2 && g.ks->E_alt == g.ks->E) continue;  // same plan as family 0
       g.pipe_cols = cf == 1;
+      g.col_family = cf;
       const float ms = time_it([&] {
         phase_col_a(g, E.base, 0, st);
         phase_col_b(g, st);
@@ -536,6 +552,7 @@ esc_status autotune(Engine& E) {
       }
     }
     g.pipe_cols = can_pipe_cols;
+    g.col_family = -1;
     apply_cols(g, best_cf);
     float best_r = 1e30f;
     int best_rf = 0;
@@ -584,8 +601,41 @@ void launch_step(Engine& E, int s_local, cudaStream_t st) {
 esc_status ensure_graph(Engine& E) {
   if (E.gexec) return ESC_OK;
   cudaGraph_t graph = nullptr;
+  // The size groups are independent for a whole chunk: each group's chain of
+  // kChunk steps is captured on its own forked stream, so the chains overlap and
+  // fill each other's launch tails; they join before the step counter advances.
+  const int ng = (int)E.groups.size();
+  if ((int)E.side.size() < ng) {
+    for (int i = (int)E.side.size(); i < ng; ++i) {
+      cudaStream_t s = nullptr;
+      CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      E.side.push_back(s);
+      cudaEvent_t ev = nullptr;
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      E.side_ev.push_back(ev);
+    }
+    if (!E.fork_ev) CK(cudaEventCreateWithFlags(&E.fork_ev, cudaEventDisableTiming));
+  }
+  const char* fork_env = getenv("ESC_GRAPH_FORK");
+  const bool fork = !(fork_env && fork_env[0] == '0') && ng > 1;
   CK(cudaStreamBeginCapture(E.own, cudaStreamCaptureModeThreadLocal));
-  for (int s = 0; s < kChunk; ++s) launch_step(E, s, E.own);
+  if (!fork) {
+    for (int s = 0; s < kChunk; ++s) launch_step(E, s, E.own);
+  }
+  CK(cudaEventRecord(E.fork_ev, E.own));
+  for (int gi = 0; fork && gi < ng; ++gi) {
+    cudaStream_t ss = E.side[gi];
+    CK(cudaStreamWaitEvent(ss, E.fork_ev, 0));
+    Group& g = E.groups[gi];
+    for (int s = 0; s < kChunk; ++s) {
+      phase_row_a(g, E.base, s, ss);
+      phase_col_a(g, E.base, s, ss);
+      phase_row_b(g, E.base, s, ss);
+      phase_col_b(g, ss);
+    }
+    CK(cudaEventRecord(E.side_ev[gi], ss));
+    CK(cudaStreamWaitEvent(E.own, E.side_ev[gi], 0));
+  }
   k_advance<<<1, 32, 0, E.own>>>(E.base, kChunk);
   const cudaError_t ec = cudaStreamEndCapture(E.own, &graph);
   if (ec != cudaSuccess) {
@@ -970,6 +1020,7 @@ esc_status esc_create(esc_ctx** out, int n, double dx, const double* phi, const 
   const double* phis[1] = {phi};
   esc_status s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
   if (s == ESC_OK) s = autotune(c->e);
+  if (s == ESC_OK) s = ensure_graph(c->e);
   if (s != ESC_OK) {
     tl_err = c->e.err;
     c->e.release();
@@ -1036,6 +1087,7 @@ esc_status esc_batch_create(esc_batch** out, int count, const int* n, const doub
   }
   esc_status s = engine_create(b->e, count, n, dx, phi, p, (int)prec);
   if (s == ESC_OK) s = autotune(b->e);
+  if (s == ESC_OK) s = ensure_graph(b->e);
   if (s != ESC_OK) {
     tl_err = b->e.err;
     b->e.release();
@@ -1148,16 +1200,16 @@ int esc_batch_describe(const esc_batch* b, char* buf, int buflen) {
   if (!b) return -1;
   std::string out = "[";
   static const char* rows[3] = {"block", "tma-pipeline", "warp"};
-  static const char* cols[2] = {"block", "tma-pipeline"};
+  static const char* cols[3] = {"block", "tma-pipeline", "block-alt-plan"};
   for (size_t i = 0; i < b->e.groups.size(); ++i) {
     const Group& g = b->e.groups[i];
     char tmp[512];
     snprintf(tmp, sizeof tmp,
              "%s{\"n\": %d, \"instances\": %zu, \"rows\": \"%s\", \"cols\": \"%s\", \"row_ms\": [%.4f, %.4f, %.4f], "
-             "\"col_ms\": [%.4f, %.4f], \"E\": %d}",
+             "\"col_ms\": [%.4f, %.4f, %.4f], \"E\": %d, \"E_alt\": %d}",
              i ? ", " : "", g.n, g.members.size(), g.row_family >= 0 ? rows[g.row_family] : "?",
              g.col_family >= 0 ? cols[g.col_family] : "?", g.row_ms[0], g.row_ms[1], g.row_ms[2], g.col_ms[0],
-             g.col_ms[1], g.ks->E);
+             g.col_ms[1], g.col_ms[2], g.ks->E, g.ks->E_alt);
     out += tmp;
   }
   out += "]";

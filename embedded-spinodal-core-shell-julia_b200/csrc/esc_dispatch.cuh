@@ -35,6 +35,10 @@ struct KernelSet {
   void (*row_a_w)(const InstDev*, int, const int*, int, cudaStream_t);
   void (*row_b_w)(const InstDev*, int, const int*, int, cudaStream_t);
   cudaError_t (*prepare_warp)();
+  // column kernels with the alternative (fewer elements per thread) plan
+  void (*col_a_alt)(const InstDev*, int, const int*, int, cudaStream_t);
+  void (*col_b_alt)(const InstDev*, int, cudaStream_t);
+  int E_alt;
   // adjoint step kernels (FP64 kernel sets only; null in the mixed sets)
   cudaError_t (*prepare_adj)();
   void (*adj_col1)(const AdjDev*, int, cudaStream_t);
@@ -43,6 +47,23 @@ struct KernelSet {
   void (*adj_mu_col)(const AdjDev*, int, cudaStream_t);
   void (*adj_seed_row)(const AdjDev*, int, cudaStream_t);
 };
+
+// Alternative column plans: fewer elements per thread (more passes, fewer
+// registers, more resident warps).  The autotuner times them against the
+// default plan.
+template <int N>
+struct AltPlan {
+  using type = typename DefaultPlan<N>::type;
+};
+#define ESC_ALTPLAN(n, e, ...) \
+  template <>                  \
+  struct AltPlan<n> { using type = Plan<n, e, Radices<__VA_ARGS__>>; };
+ESC_ALTPLAN(128, 8, 4, 4, 8)
+ESC_ALTPLAN(256, 8, 4, 8, 8)
+ESC_ALTPLAN(384, 12, 6, 4, 4, 4)
+ESC_ALTPLAN(768, 12, 12, 4, 4, 4)
+ESC_ALTPLAN(1024, 8, 4, 4, 8, 8)
+#undef ESC_ALTPLAN
 
 // FP64 plans keep E <= 16 so that two register arrays of double2 fit.
 template <int N>
@@ -88,7 +109,7 @@ struct KS {
       return e;
     if ((e = cudaFuncSetAttribute(k_col_b<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
       return e;
-    return cudaSuccess;
+    return prepare_alt();
   }
   static void init(const InstDev* d, int count, cudaStream_t st) {
     k_init<P, SR><<<dim3(tiles_pairs, count), kBlock, smem(), st>>>(d);
@@ -217,6 +238,28 @@ struct KS {
     if constexpr (warp_ok)
       k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kBlock, warp_smem(), st>>>(d, base, s);
   }
+  // ---- alternative column plan ----
+  using AP = typename AltPlan<N>::type;
+  static constexpr int alt_tiles_cols = (H + kBlock / AP::T - 1) / (kBlock / AP::T);
+  static size_t alt_smem() {
+    constexpr int Ga = kBlock / AP::T, Wa = kBlock / AP::T;
+    const size_t row = (size_t)Ga * RowLayout<N>::stride;
+    const size_t col = (size_t)host_smpad(N * Wa - 1) + 1;
+    return (row > col ? row : col) * sizeof(cpx<SR>);
+  }
+  static cudaError_t prepare_alt() {
+    const int b = (int)alt_smem();
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_col_a<AP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_col_b<AP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    return cudaSuccess;
+  }
+  static void col_a_alt(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
+    k_col_a<AP, SR, WR><<<dim3(alt_tiles_cols, count), kBlock, alt_smem(), st>>>(d, base, s);
+  }
+  static void col_b_alt(const InstDev* d, int count, cudaStream_t st) {
+    k_col_b<AP, SR, WR><<<dim3(alt_tiles_cols, count), kBlock, alt_smem(), st>>>(d);
+  }
   // ---- adjoint (FP64) ----
   static constexpr bool adj_ok = std::is_same<SR, double>::value && std::is_same<WR, double>::value;
   static cudaError_t prepare_adj() {
@@ -259,6 +302,10 @@ struct KS {
     {
       // partial sums are scratch of one launch; size for the largest user
       int need = 5 * tiles_pairs + (tiles_cols > PG::tiles_cols ? tiles_cols : PG::tiles_cols) + tiles_rows;
+      // the alternative column plan's partials sit after 5 * (its own row tiles)
+      const int alt_need = 5 * ((H + kBlock / AP::T - 1) / (kBlock / AP::T)) + alt_tiles_cols +
+                           (N + kBlock / AP::T - 1) / (kBlock / AP::T);
+      if (alt_need > need) need = alt_need;
       const int wa = 5 * warp_tiles_pairs() * (kBlock / 32), wb = warp_tiles_rows() * (kBlock / 32);
       if (wa > need) need = wa;
       if (wb > need) need = wb;
@@ -288,6 +335,9 @@ struct KS {
     k.row_b_w = &row_b_w;
     k.prepare_warp = &prepare_warp;
     k.prepare_adj = &prepare_adj;
+    k.col_a_alt = &col_a_alt;
+    k.col_b_alt = &col_b_alt;
+    k.E_alt = AP::E;
     k.adj_col1 = adj_ok ? &adj_col1 : nullptr;
     k.adj_col2 = adj_ok ? &adj_col2 : nullptr;
     k.adj_row2 = adj_ok ? &adj_row2 : nullptr;
