@@ -20,6 +20,35 @@
 
 namespace esc {
 
+// Two FP32 lanes processed by one packed sm_100 instruction (FADD2 / FMUL2 /
+// FFMA2).  Every lane is rounded exactly like the scalar FP32 operation.  PTX
+// has no packed negation, so a - b is fma(b, -1, a) (exact product, one
+// rounding: identical to a subtraction) and -a is a * -1.
+struct __align__(8) f2 {
+  float2 v;
+  f2() = default;
+  __device__ __forceinline__ constexpr f2(float a, float b) : v{a, b} {}
+  __device__ __forceinline__ explicit constexpr f2(double s) : v{(float)s, (float)s} {}
+};
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) {
+  f2 r;
+  r.v = __fadd2_rn(a.v, b.v);
+  return r;
+}
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) {
+  f2 r;
+  r.v = __fmul2_rn(a.v, b.v);
+  return r;
+}
+using ::fma;  // keep the scalar overloads visible beside the packed one
+__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) {
+  f2 r;
+  r.v = __ffma2_rn(a.v, b.v, c.v);
+  return r;
+}
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) { return fma(b, f2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ f2 operator-(f2 a) { return a * f2(-1.0f, -1.0f); }
+
 template <typename R>
 struct __align__(2 * sizeof(R)) cpx {
   R x, y;

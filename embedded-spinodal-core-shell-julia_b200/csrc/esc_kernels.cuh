@@ -192,6 +192,46 @@ __device__ __forceinline__ void bulk(SR c, SR phi, const ModelParams& p, SR& fpr
   fbulk = A * ((SR)1 - h) * d_a * d_a + B * h * d_b * d_b * d_c * d_c + P * ((SR)1 - chi * c) * g;
 }
 
+// Bulk terms of the mixed precision for two points at once (rows a and b of a
+// row pair, one packed lane each).  c arrives in FP64; f'(c) and f(c) are
+// evaluated in FP32 at c_hi = fl32(c) and corrected to first order in
+// c_lo = fl32(c - c_hi), the part of c below FP32 resolution:
+//   f'(c) = f'(c_hi) + f''(c_hi) c_lo,   f(c) = f(c_hi) + f'(c_hi) c_lo.
+// The neglected terms are O(c_lo^2) ~ 1e-15 relative.  Same formulas as `bulk`
+// (core_shell.jl:45-55), with f'' = 2A(1-h) + 2Bh((c-cc)e + (c-cb)e + 2(c-cb)(c-cc)),
+// e = 2c - cb - cc.
+__device__ __forceinline__ void bulk_pair_split(double ca, double cb, float pa, float pb, const ModelParams& p,
+                                                f2& fprime, f2& fbulk) {
+  const f2 hi(__double2float_rn(ca), __double2float_rn(cb));
+  const f2 lo(__double2float_rn(ca - (double)hi.v.x), __double2float_rn(cb - (double)hi.v.y));
+  const f2 ph(pa, pb);
+  const f2 p2 = ph * ph;
+  const f2 h = p2 * ph * fma(ph, fma(ph, f2(6.0), f2(-15.0)), f2(10.0));
+  const f2 q = ph - p2;
+  const f2 g = q * q;
+  const f2 Ah = f2(p.A) * (f2(1.0) - h);
+  const f2 Bh = f2(p.B) * h;
+  const f2 da = hi - f2(p.ca), db = hi - f2(p.cb), dc = hi - f2(p.cc);
+  const f2 e = hi + hi - f2(p.cb + p.cc);
+  const f2 dbdc = db * dc;
+  const f2 fp = fma(f2(2.0) * Ah, da, fma(f2(2.0) * Bh * dbdc, e, f2(-p.chi * p.P) * g));
+  const f2 fpp = fma(f2(2.0), Ah, f2(2.0) * Bh * fma(dc + db, e, f2(2.0) * dbdc));
+  const f2 fv = fma(Ah * da, da, fma(Bh * dbdc, dbdc, f2(p.P) * fma(f2(-p.chi), hi, f2(1.0)) * g));
+  fprime = fma(fpp, lo, fp);
+  fbulk = fma(fp, lo, fv);
+}
+
+// true when x is +-Inf or NaN (exponent bits all set), by integer test
+__device__ __forceinline__ bool nonfinite_bits(double x) {
+  return (__double2hiint(x) & 0x7ff00000) == 0x7ff00000;
+}
+
+// L1 prefetch of `bytes` bytes from `p` (128-byte lines), lines split over `nthr` threads
+__device__ __forceinline__ void prefetch_l1(const void* p, int bytes, int t, int nthr) {
+  const char* c = static_cast<const char*>(p);
+  for (int l = t; l * 128 < bytes; l += nthr) asm volatile("prefetch.global.L1 [%0];" ::"l"(c + 128 * l));
+}
+
 template <typename R>
 __device__ __forceinline__ R mobility_of(R phi, R M0) {
   return M0 * (phi * phi * phi * ((R)10 - (R)15 * phi + (R)6 * phi * phi));

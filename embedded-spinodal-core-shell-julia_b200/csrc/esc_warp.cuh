@@ -10,7 +10,13 @@
 #pragma once
 #include "esc_pipe.cuh"
 
+#include <type_traits>
+
 namespace esc {
+
+// the mixed precision: FP64 state transforms, FP32 flux transforms
+template <typename SR, typename WR>
+constexpr bool kSplitMixed = std::is_same<SR, double>::value && std::is_same<WR, float>::value;
 
 // Plans with every group inside a warp (T <= 32) and E <= 16 where possible.
 template <int N>
@@ -105,6 +111,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_row_a_w(const InstDev* __restrict
 
   cpx<SR> v[E];
   if (active) {
+    prefetch_l1(reinterpret_cast<const WR*>(I.phi) + (size_t)ya * N, 2 * N * (int)sizeof(WR), t, T);
     const cpx<SR>* S = reinterpret_cast<const cpx<SR>*>(I.S);
     const cpx<SR>* ra = S + (size_t)ya * H;
     const cpx<SR>* rb = ra + H;
@@ -125,6 +132,28 @@ __global__ void __launch_bounds__(kBlock, 2) k_row_a_w(const InstDev* __restrict
   const WR* phi = reinterpret_cast<const WR*>(I.phi);
   double sum_c = 0.0, sum_f = 0.0, mn = INFINITY, mx = -INFINITY, bad = 0.0;
   cpx<WR> wv[E];
+  if constexpr (kSplitMixed<SR, WR>) {
+    // FP32 bulk terms with the FP64 remainder of c folded in to first order
+    int nbad = 0;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int x = t + T * m;
+      f2 fp(0.0f, 0.0f);
+      if (active) {
+        const double ca = v[m].x * invN, cb = v[m].y * invN;
+        f2 fv;
+        bulk_pair_split(ca, cb, __ldg(reinterpret_cast<const float*>(phi) + (size_t)ya * N + x),
+                        __ldg(reinterpret_cast<const float*>(phi) + (size_t)(ya + 1) * N + x), mp, fp, fv);
+        sum_c += ca + cb;
+        sum_f += (double)(fv.v.x + fv.v.y);
+        mn = fmin(mn, fmin(ca, cb));
+        mx = fmax(mx, fmax(ca, cb));
+        nbad += (int)(nonfinite_bits(ca) | nonfinite_bits(cb));
+      }
+      wv[m] = mkc<WR>((WR)fp.v.x, (WR)fp.v.y);
+    }
+    bad = (double)nbad;
+  } else {
 #pragma unroll
   for (int m = 0; m < E; ++m) {
     const int x = t + T * m;
@@ -142,6 +171,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_row_a_w(const InstDev* __restrict
       bad += (isfinite((double)ca) ? 0.0 : 1.0) + (isfinite((double)cb) ? 0.0 : 1.0);
     }
     wv[m] = mkc<WR>((WR)fa, (WR)fb);
+  }
   }
   cpx<WR>* xw = reinterpret_cast<cpx<WR>*>(smraw);
   // the FP32 exchange reuses the group's slice (n elements of the smaller type)
@@ -215,6 +245,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_row_b_w(const InstDev* __restrict
   cpx2<WR>* row = reinterpret_cast<cpx2<WR>*>(I.G) + (size_t)(active ? y : 0) * H;
   cpx<WR> v[E];
   if (active) {
+    prefetch_l1(reinterpret_cast<const WR*>(I.phi) + (size_t)y * N, N * (int)sizeof(WR), t, T);
     load_pair_rows<P, WR>(v, t, [&](int idx, cpx<WR>& a, cpx<WR>& b) {
       const cpx2<WR> q = row[idx];
       a = q.a;
