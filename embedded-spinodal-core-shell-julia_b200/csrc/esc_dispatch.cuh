@@ -227,6 +227,8 @@ struct KS {
       const int b = (int)warp_smem();
       if ((e = cudaFuncSetAttribute(k_row_a_w<WP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
       if ((e = cudaFuncSetAttribute(k_row_b_w<WP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+      if constexpr (kPackedRows)
+        if ((e = cudaFuncSetAttribute(k_row_b_w2<WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
     }
     return cudaSuccess;
   }
@@ -234,9 +236,15 @@ struct KS {
     if constexpr (warp_ok)
       k_row_a_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kBlock, warp_smem(), st>>>(d, base, s);
   }
+  // the mixed precision transforms two rows per group in packed FP32 pairs
+  static constexpr bool kPackedRows = std::is_same<SR, double>::value && std::is_same<WR, float>::value;
   static void row_b_w(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
-    if constexpr (warp_ok)
-      k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kBlock, warp_smem(), st>>>(d, base, s);
+    if constexpr (warp_ok) {
+      if constexpr (kPackedRows)
+        k_row_b_w2<WP><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kBlock, warp_smem(), st>>>(d, base, s);
+      else
+        k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kBlock, warp_smem(), st>>>(d, base, s);
+    }
   }
   // ---- alternative column plan ----
   using AP = typename AltPlan<N>::type;

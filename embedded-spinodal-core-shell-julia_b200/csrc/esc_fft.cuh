@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace esc {
 
 // Two FP32 lanes processed by one packed sm_100 instruction (FADD2 / FMUL2 /
@@ -98,6 +100,28 @@ __device__ __forceinline__ cpx<double> ldc<double>(const cpx<double>* p) {
   return mkc<double>(v.x, v.y);
 }
 
+// ---- packed pairs of complex values: cpx<f2> holds (x0, x1) + i (y0, y1), two
+// independent transforms in the two lanes.  Twiddle tables for them hold each
+// factor duplicated in both lanes.
+template <>
+__device__ __forceinline__ cpx<f2> ldc<f2>(const cpx<f2>* p) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  return mkc<f2>(f2(v.x, v.y), f2(v.z, v.w));
+}
+__device__ __forceinline__ cpx<f2> cmul(cpx<f2> a, cpx<f2> b) {
+  const f2 nby = b.y * f2(-1.0f, -1.0f);
+  return mkc<f2>(fma(a.y, nby, a.x * b.x), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ cpx<f2> cmulconj(cpx<f2> a, cpx<f2> b) {  // a * conj(b)
+  const f2 nby = b.y * f2(-1.0f, -1.0f);
+  return mkc<f2>(fma(a.y, b.y, a.x * b.x), fma(a.x, nby, a.y * b.x));
+}
+__device__ __forceinline__ cpx<f2> pack2(cpx<float> a, cpx<float> b) {
+  return mkc<f2>(f2(a.x, b.x), f2(a.y, b.y));
+}
+__device__ __forceinline__ cpx<float> lane0(cpx<f2> v) { return mkc<float>(v.x.v.x, v.y.v.x); }
+__device__ __forceinline__ cpx<float> lane1(cpx<f2> v) { return mkc<float>(v.x.v.y, v.y.v.y); }
+
 // cos / sin of 2*pi*a/48 for the multiples used by the in-register radices
 // (6, 8, 12, 16 all divide 48).  Correctly rounded double constants.
 __device__ __forceinline__ constexpr double cos48(int a) {
@@ -142,7 +166,12 @@ __device__ __forceinline__ cpx<Re> twiddle_const(cpx<Re> v, int e) {
   const int a = e * (48 / R);
   const Re c = (Re)cos48(a);
   const Re s = INV ? (Re)sin48(a) : -(Re)sin48(a);
-  return mkc<Re>(fma(v.x, c, -v.y * s), fma(v.x, s, v.y * c));
+  if constexpr (std::is_same<Re, f2>::value) {
+    const Re ns = INV ? (Re)-sin48(a) : (Re)sin48(a);  // no packed negation: fold the sign into the constant
+    return mkc<Re>(fma(v.y, ns, v.x * c), fma(v.x, s, v.y * c));
+  } else {
+    return mkc<Re>(fma(v.x, c, -v.y * s), fma(v.x, s, v.y * c));
+  }
 }
 
 // ---- small DFTs in registers -------------------------------------------------
@@ -166,7 +195,8 @@ struct DFT<3, INV, Re> {
     const cpx<Re> t2 = mkc<Re>(fma((Re)-0.5, t1.x, b[0].x), fma((Re)-0.5, t1.y, b[0].y));
     const cpx<Re> d = b[1] - b[2];
     // forward: X1 = t2 - i h d, X2 = t2 + i h d ; inverse swaps the sign of i
-    const cpx<Re> ihd = mkc<Re>(-h * d.y, h * d.x);  // i*h*d
+    const Re nh = (Re)-8.660254037844385965883e-01;
+    const cpx<Re> ihd = mkc<Re>(nh * d.y, h * d.x);  // i*h*d
     b[0] = b[0] + t1;
     if (INV) {
       b[1] = t2 + ihd;
@@ -183,11 +213,17 @@ struct DFT<4, INV, Re> {
   static __device__ __forceinline__ void run(cpx<Re>* b) {
     const cpx<Re> s02 = b[0] + b[2], d02 = b[0] - b[2];
     const cpx<Re> s13 = b[1] + b[3], d13 = b[1] - b[3];
-    const cpx<Re> r = INV ? times_i(d13) : times_negi(d13);
+    // b[1] = d02 + r, b[3] = d02 - r with r = -i d13 (forward) or +i d13
+    // (inverse), written component-wise so that no negation is needed
     b[0] = s02 + s13;
     b[2] = s02 - s13;
-    b[1] = d02 + r;
-    b[3] = d02 - r;
+    if (INV) {
+      b[1] = mkc<Re>(d02.x - d13.y, d02.y + d13.x);
+      b[3] = mkc<Re>(d02.x + d13.y, d02.y - d13.x);
+    } else {
+      b[1] = mkc<Re>(d02.x + d13.y, d02.y - d13.x);
+      b[3] = mkc<Re>(d02.x - d13.y, d02.y + d13.x);
+    }
   }
 };
 
@@ -298,10 +334,14 @@ struct WarpSync {
   static __device__ __forceinline__ void sync() { __syncwarp(); }
 };
 
+// Twiddle factor j of a table e^{-2 pi i j / N} in global memory (read through
+// the non-coherent path).
+template <typename Re>
+__device__ __forceinline__ cpx<Re> tw_at(const cpx<Re>* tw, int i) { return ldc(tw + i); }
+
 // One Stockham pass (radix RAD, NS = product of earlier radices).
-template <bool INV, class P, int RAD, int NS, bool LAST, class Sync = BlockSync, typename Re, class L>
-__device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
-                                              const cpx<Re>* __restrict__ tw) {
+template <bool INV, class P, int RAD, int NS, bool LAST, class Sync = BlockSync, typename Re, class L, class TW>
+__device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay, const TW& tw) {
   constexpr int N = P::N, E = P::E, T = P::T;
   constexpr int NB = E / RAD;
   static_assert(E % RAD == 0, "radix must divide E");
@@ -316,7 +356,7 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
       constexpr int STEP = N / (NS * RAD);
 #pragma unroll
       for (int s = 1; s < RAD; ++s) {
-        const cpx<Re> w = ldc(tw + s * k * STEP);
+        const cpx<Re> w = tw_at(tw, s * k * STEP);
         b[s] = INV ? cmulconj(b[s], w) : cmul(b[s], w);
       }
     }
@@ -338,9 +378,9 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
   }
 }
 
-template <bool INV, class P, int NS, class Sync, typename Re, class L, int RAD, int... REST>
-__device__ __forceinline__ void fft_passes(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
-                                           const cpx<Re>* __restrict__ tw, Radices<RAD, REST...>) {
+template <bool INV, class P, int NS, class Sync, typename Re, class L, class TW, int RAD, int... REST>
+__device__ __forceinline__ void fft_passes(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay, const TW& tw,
+                                           Radices<RAD, REST...>) {
   constexpr bool LAST = sizeof...(REST) == 0;
   stockham_pass<INV, P, RAD, NS, LAST, Sync>(v, t, sm, lay, tw);
   if constexpr (!LAST) fft_passes<INV, P, NS * RAD, Sync>(v, t, sm, lay, tw, Radices<REST...>{});
@@ -349,9 +389,8 @@ __device__ __forceinline__ void fft_passes(cpx<Re> (&v)[P::E], int t, cpx<Re>* s
 // Length-N DFT of the values v[m] at positions t + T*m; result in the same slots.
 // tw: table of e^{-2 pi i j / N}, j < N, in global memory (read through L1).
 // Every thread of the CTA must call this (it contains __syncthreads).
-template <bool INV, class P, class Sync = BlockSync, typename Re, class L>
-__device__ __forceinline__ void fft(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay,
-                                    const cpx<Re>* __restrict__ tw) {
+template <bool INV, class P, class Sync = BlockSync, typename Re, class L, class TW>
+__device__ __forceinline__ void fft(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay, const TW& tw) {
   fft_passes<INV, P, 1, Sync>(v, t, sm, lay, tw, typename P::List{});
 }
 

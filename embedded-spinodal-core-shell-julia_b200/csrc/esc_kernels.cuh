@@ -56,6 +56,7 @@ struct InstDev {
   long long* bad_step;
   const void* tw_s;   // twiddles e^{-2 pi i j/n} in SR
   const void* tw_w;   // same in WR
+  const void* tw_p;   // FP32 table with each factor in both lanes of a packed pair (mixed only)
   double* cio;        // real FP64 field for init/final (n*n)
 };
 

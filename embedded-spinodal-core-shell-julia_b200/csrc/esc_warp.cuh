@@ -295,4 +295,122 @@ __global__ void __launch_bounds__(kBlock, 2) k_row_b_w(const InstDev* __restrict
   }
 }
 
+// =====================================================================================
+// Packed row B of the mixed precision: each group transforms two adjacent rows
+// at once, one per lane of packed FP32 pairs (cpx<f2>), so every butterfly
+// instruction serves both rows and a warp keeps twice the data in flight.
+// The numerics are those of k_row_b_w per lane, except that the 1/2 of the
+// two-real-fields split is folded into the mobility (an exact scaling).
+
+// Split of the packed DFTs Y = FFT(a + i b) (one per lane) into the packed half
+// spectra of a and b, when the data already carry the factor 1/2:
+//   Xa(k) = Y(k) + conj Y(n-k),  Xb(k) = -i (Y(k) - conj Y(n-k)),
+// slot k = 0 of thread 0 packing (DC, Nyquist) at full scale.
+template <class P>
+__device__ __forceinline__ void split_rows_packed(const cpx<f2> (&y)[P::E], int t, cpx<f2> (&xa)[P::E / 2],
+                                                  cpx<f2> (&xb)[P::E / 2]) {
+  constexpr int E = P::E, T = P::T;
+  static_assert(T <= 32, "mirror exchange by shuffle");
+  const int lane = threadIdx.x & 31;
+  const int src = lane - t + ((T - t) & (T - 1));
+#pragma unroll
+  for (int m = 0; m < E / 2; ++m) {
+    const cpx<f2> q = y[E - 1 - m];
+    cpx<f2> y2;
+    y2.x.v.x = __shfl_sync(0xffffffffu, q.x.v.x, src);
+    y2.x.v.y = __shfl_sync(0xffffffffu, q.x.v.y, src);
+    y2.y.v.x = __shfl_sync(0xffffffffu, q.y.v.x, src);
+    y2.y.v.y = __shfl_sync(0xffffffffu, q.y.v.y, src);
+    const cpx<f2> y1 = y[m];
+    if (t == 0) {
+      if (m == 0) {
+        const cpx<f2> yh = y[E / 2];
+        xa[0] = mkc<f2>(y1.x + y1.x, yh.x + yh.x);
+        xb[0] = mkc<f2>(y1.y + y1.y, yh.y + yh.y);
+        continue;
+      }
+      y2 = y[E - m];
+    }
+    xa[m] = mkc<f2>(y1.x + y2.x, y1.y - y2.y);
+    xb[m] = mkc<f2>(y1.y + y2.y, y2.x - y1.x);
+  }
+}
+
+template <class P>
+__global__ void __launch_bounds__(kBlock, 2) k_row_b_w2(const InstDev* __restrict__ insts,
+                                                        const int* __restrict__ base, int s_local) {
+  using WG = WarpRowGeom<P>;
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
+  constexpr int tiles = WG::tiles_pairs;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const InstDev& I = insts[blockIdx.y];
+  if (!warp_instance_running(I.status)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = lane % T, gw = lane / T;
+  const int g = warp * GPW + gw;
+  const int pair = blockIdx.x * G + g;
+  const bool active = pair < H;
+  const int y0 = 2 * (active ? pair : 0);
+  cpx2<float>* r0 = reinterpret_cast<cpx2<float>*>(I.G) + (size_t)y0 * H;
+  cpx2<float>* r1 = r0 + H;
+  const float* phi = reinterpret_cast<const float*>(I.phi) + (size_t)y0 * N;
+  cpx<f2> v[E];
+  if (active) {
+    prefetch_l1(phi, 2 * N * (int)sizeof(float), t, T);
+    load_pair_rows<P, f2>(v, t, [&](int idx, cpx<f2>& a, cpx<f2>& b) {
+      const cpx2<float> q0 = r0[idx], q1 = r1[idx];
+      a = pack2(q0.a, q1.a);
+      b = pack2(q0.b, q1.b);
+    });
+  } else {
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = mkc<f2>(f2(0.0f, 0.0f), f2(0.0f, 0.0f));
+  }
+  cpx<f2>* xs = reinterpret_cast<cpx<f2>*>(smraw);
+  const SwizzleLayout<N, sizeof(cpx<f2>)> lay{g * N, gw};
+  const cpx<f2>* twp = reinterpret_cast<const cpx<f2>*>(I.tw_p);
+  fft<true, P, WarpSync>(v, t, xs, lay, twp);
+  const f2 Mh(0.5 * I.p.mobility);
+  double dsum = 0.0;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    f2 M(0.0f, 0.0f);
+    if (active) {
+      const int x = t + T * m;
+      const f2 ph(__ldg(phi + x), __ldg(phi + N + x));
+      const f2 p2 = ph * ph;
+      M = Mh * (p2 * ph * fma(ph, fma(ph, f2(6.0), f2(-15.0)), f2(10.0)));
+      const f2 d = M * fma(v[m].x, v[m].x, v[m].y * v[m].y);
+      dsum += (double)d.v.x + (double)d.v.y;
+    }
+    v[m] = mkc<f2>(v[m].x * M, v[m].y * M);
+  }
+  __syncwarp();  // every lane of the group has finished its gathers before the next scatter
+  fft<false, P, WarpSync>(v, t, xs, lay, twp);
+  cpx<f2> xa[E / 2], xb[E / 2];
+  split_rows_packed<P>(v, t, xa, xb);
+  if (active) {
+#pragma unroll
+    for (int m = 0; m < E / 2; ++m) {
+      cpx2<float> o0, o1;
+      o0.a = lane0(xa[m]);
+      o0.b = lane0(xb[m]);
+      o1.a = lane1(xa[m]);
+      o1.b = lane1(xb[m]);
+      r0[t + T * m] = o0;
+      r1[t + T * m] = o1;
+    }
+  }
+  dsum = 2.0 * warp_sum(dsum);
+  const int slot = blockIdx.x * NW + warp;
+  if (lane == 0) I.part[slot] = dsum;
+  if (!warp_arrive_last(&I.cnt[2], (unsigned)(tiles * NW))) return;
+  const double d = warp_fold<OpSum>(I.part, tiles * NW, 1, 0.0);
+  if (lane == 0) {
+    const int s = step_index(base, s_local);
+    if (I.hist) I.hist[s + 5 * (size_t)I.hist_ld] = d * I.dx * I.dx;
+    I.cnt[2] = 0;
+  }
+}
+
 }  // namespace esc
