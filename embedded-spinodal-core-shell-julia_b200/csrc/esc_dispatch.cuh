@@ -60,8 +60,8 @@ struct AltPlan {
   struct AltPlan<n> { using type = Plan<n, e, Radices<__VA_ARGS__>>; };
 ESC_ALTPLAN(128, 8, 4, 4, 8)
 ESC_ALTPLAN(256, 8, 4, 8, 8)
-ESC_ALTPLAN(384, 12, 6, 4, 4, 4)
-ESC_ALTPLAN(768, 12, 12, 4, 4, 4)
+ESC_ALTPLAN(384, 12, 4, 4, 4, 6)
+ESC_ALTPLAN(768, 12, 4, 4, 4, 12)
 ESC_ALTPLAN(1024, 8, 4, 4, 8, 8)
 #undef ESC_ALTPLAN
 
@@ -73,11 +73,11 @@ struct Plan64 {
 #define ESC_PLAN64(n, e, ...) \
   template <>                 \
   struct Plan64<n> { using type = Plan<n, e, Radices<__VA_ARGS__>>; };
-ESC_PLAN64(96, 12, 6, 4, 4)
-ESC_PLAN64(384, 12, 6, 4, 4, 4)
-ESC_PLAN64(768, 12, 12, 4, 4, 4)
-ESC_PLAN64(1536, 12, 6, 4, 4, 4, 4)
-ESC_PLAN64(3072, 12, 12, 4, 4, 4, 4)
+ESC_PLAN64(96, 12, 4, 4, 6)
+ESC_PLAN64(384, 12, 4, 4, 4, 6)
+ESC_PLAN64(768, 12, 4, 4, 4, 12)
+ESC_PLAN64(1536, 12, 4, 4, 4, 4, 6)
+ESC_PLAN64(3072, 12, 4, 4, 4, 4, 12)
 #undef ESC_PLAN64
 
 inline int host_smpad(int p) { return p + (p >> 4); }

@@ -282,29 +282,32 @@ struct Plan {
 };
 
 // Default plans: E elements per thread, radix sequence (each radix divides E).
+// Radices 3, 6 and 12 come last: the last pass exchanges nothing, and every
+// earlier pass then has power-of-two strides, which the swizzled exchange
+// layout keeps free of shared-memory bank conflicts.
 template <int N>
 struct DefaultPlan;
 #define ESC_PLAN(n, e, ...) \
   template <>               \
   struct DefaultPlan<n> { using type = Plan<n, e, Radices<__VA_ARGS__>>; };
 ESC_PLAN(8, 8, 8)
-ESC_PLAN(12, 12, 3, 4)
+ESC_PLAN(12, 12, 4, 3)
 ESC_PLAN(16, 16, 16)
-ESC_PLAN(24, 12, 3, 4, 2)
+ESC_PLAN(24, 12, 4, 2, 3)
 ESC_PLAN(32, 8, 4, 8)
-ESC_PLAN(48, 12, 3, 4, 4)
+ESC_PLAN(48, 12, 4, 4, 3)
 ESC_PLAN(64, 8, 8, 8)
-ESC_PLAN(96, 24, 3, 4, 8)
+ESC_PLAN(96, 24, 4, 8, 3)
 ESC_PLAN(128, 16, 8, 16)
-ESC_PLAN(192, 12, 3, 4, 4, 4)
+ESC_PLAN(192, 12, 4, 4, 4, 3)
 ESC_PLAN(256, 16, 16, 16)
-ESC_PLAN(384, 24, 6, 8, 8)
+ESC_PLAN(384, 24, 8, 8, 6)
 ESC_PLAN(512, 8, 8, 8, 8)
-ESC_PLAN(768, 24, 12, 8, 8)
+ESC_PLAN(768, 24, 8, 8, 12)
 ESC_PLAN(1024, 16, 4, 16, 16)
-ESC_PLAN(1536, 24, 3, 8, 8, 8)
+ESC_PLAN(1536, 24, 8, 8, 8, 3)
 ESC_PLAN(2048, 16, 8, 16, 16)
-ESC_PLAN(3072, 24, 6, 8, 8, 8)
+ESC_PLAN(3072, 24, 8, 8, 8, 6)
 ESC_PLAN(4096, 16, 16, 16, 16)
 #undef ESC_PLAN
 
@@ -313,16 +316,22 @@ __device__ __forceinline__ int smpad(int p) { return p + (p >> 4); }
 
 // Exchange addressing.  Row layout: group g owns a padded region of N elements;
 // Col layout: element p of column w sits at linear index p*W + w (then padded).
+// `at<RAD, NS>(p)` is the address used by the exchange after a pass of radix
+// RAD with NS = product of the earlier radices (scatter and gather alike).
 template <int N>
 struct RowLayout {
   int base;  // g * stride
   static constexpr int stride = N + N / 16 + 1;
   __device__ __forceinline__ int operator()(int p) const { return base + smpad(p); }
+  template <int RAD, int NS>
+  __device__ __forceinline__ int at(int p) const { return (*this)(p); }
 };
 template <int W>
 struct ColLayout {
   int w;
   __device__ __forceinline__ int operator()(int p) const { return smpad(p * W + w); }
+  template <int RAD, int NS>
+  __device__ __forceinline__ int at(int p) const { return (*this)(p); }
 };
 
 // Barrier used between the scatter and gather of an exchange: the whole block,
@@ -367,13 +376,13 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
     } else {
       const int base = (j / NS) * NS * RAD + (j % NS);
 #pragma unroll
-      for (int s = 0; s < RAD; ++s) sm[lay(base + s * NS)] = b[s];
+      for (int s = 0; s < RAD; ++s) sm[lay.template at<RAD, NS>(base + s * NS)] = b[s];
     }
   }
   if (!LAST) {
     Sync::sync();
 #pragma unroll
-    for (int m = 0; m < E; ++m) v[m] = sm[lay(t + T * m)];
+    for (int m = 0; m < E; ++m) v[m] = sm[lay.template at<RAD, NS>(t + T * m)];
     Sync::sync();
   }
 }
@@ -398,6 +407,16 @@ __device__ __forceinline__ void fft(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, cons
 // swizzled inside each 128-byte line (with a per-group offset) so that the
 // strided scatters and the gathers of one warp hit distinct banks.  Requires
 // n to be a multiple of the line length; smaller or odd sizes stay linear.
+//
+// The exchange after a pass (radix RAD = 2^r, NS = 2^a) scatters element s of
+// butterfly j to p = (j >> a) << (a + r) | s << a | (j & (NS - 1)): the lanes
+// of one bank phase differ in j, whose low a bits already sit in the low bits
+// of p while the rest sit from bit a + r up.  `at` XORs bits from
+// S = max(log2 LINE, a + r) upwards into bit a and above, which lands them in
+// the bank bits that s occupies (the same for every lane of an instruction),
+// so the scatter spreads over all banks; the gather (consecutive p in a phase)
+// sees a constant XOR and stays conflict-free.  The map only permutes within a
+// line, so it is a bijection.  Other radices use the line-index swizzle.
 template <int N, int ELEM_BYTES>
 struct SwizzleLayout {
   int base;
@@ -408,6 +427,18 @@ struct SwizzleLayout {
       return base + (p ^ (((p / LINE) + 4 * g) & (LINE - 1)));
     } else {
       return base + p;
+    }
+  }
+  static constexpr int lg(int v) { return v <= 1 ? 0 : 1 + lg(v / 2); }
+  template <int RAD, int NS>
+  __device__ __forceinline__ int at(int p) const {
+    constexpr bool pow2 = (RAD & (RAD - 1)) == 0 && (NS & (NS - 1)) == 0;
+    if constexpr (N % LINE == 0 && pow2) {
+      constexpr int a = lg(NS), r = lg(RAD), LL = lg(LINE);
+      constexpr int S = (a + r > LL) ? a + r : LL;
+      return base + (p ^ ((((p >> S) << a) + 4 * g) & (LINE - 1)));
+    } else {
+      return (*this)(p);
     }
   }
 };

@@ -22,9 +22,15 @@
 #pragma once
 #include "esc_fft.cuh"
 
+#include <type_traits>
+
 namespace esc {
 
 constexpr int kBlock = 256;
+
+// the mixed precision: FP64 state transforms, FP32 flux transforms (packed in pairs where two run side by side)
+template <typename SR, typename WR>
+constexpr bool kSplitMixed = std::is_same<SR, double>::value && std::is_same<WR, float>::value;
 
 template <typename R>
 struct __align__(4 * sizeof(R)) cpx2 {
@@ -497,16 +503,34 @@ __global__ void __launch_bounds__(kBlock) k_col_a(const InstDev* __restrict__ in
   fft<false, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
   const WR scale = (WR)(1.0 / ((double)N * (double)N));
   const WR kxd = (WR)kxf;  // kx < n/2: never the Nyquist
+  if constexpr (kSplitMixed<SR, WR>) {
+    // both derivatives in one packed transform (lane 0: x, lane 1: y)
+    cpx<f2> q[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m) {
-    const int ky = t + T * m;
-    const WR kyd = (ky == H) ? (WR)0 : wavenumber<WR>(ky, N, kunit);
-    const cpx<WR> mu = cscale(a[m] + u[m], scale);
-    a[m] = times_i(cscale(mu, kxd));   // x-derivative
-    u[m] = times_i(cscale(mu, kyd));   // y-derivative
+    for (int m = 0; m < E; ++m) {
+      const int ky = t + T * m;
+      const WR kyd = (ky == H) ? (WR)0 : wavenumber<WR>(ky, N, kunit);
+      const cpx<WR> mu = cscale(a[m] + u[m], scale);
+      q[m] = pack2(times_i(cscale(mu, kxd)), times_i(cscale(mu, kyd)));
+    }
+    fft<true, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, reinterpret_cast<const cpx<f2>*>(I.tw_p));
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      a[m] = lane0(q[m]);
+      u[m] = lane1(q[m]);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int ky = t + T * m;
+      const WR kyd = (ky == H) ? (WR)0 : wavenumber<WR>(ky, N, kunit);
+      const cpx<WR> mu = cscale(a[m] + u[m], scale);
+      a[m] = times_i(cscale(mu, kxd));   // x-derivative
+      u[m] = times_i(cscale(mu, kyd));   // y-derivative
+    }
+    fft<true, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+    fft<true, P>(u, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
   }
-  fft<true, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
-  fft<true, P>(u, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
   if (active) {
     cpx2<WR>* Gp = reinterpret_cast<cpx2<WR>*>(I.G);
 #pragma unroll
@@ -618,8 +642,21 @@ __global__ void __launch_bounds__(kBlock) k_col_b(const InstDev* __restrict__ in
     }
   }
   cpx<WR>* smw = reinterpret_cast<cpx<WR>*>(smraw);
-  fft<false, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
-  fft<false, P>(b, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  if constexpr (kSplitMixed<SR, WR>) {
+    // both flux components in one packed transform (lane 0: x, lane 1: y)
+    cpx<f2> q[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) q[m] = pack2(a[m], b[m]);
+    fft<false, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, reinterpret_cast<const cpx<f2>*>(I.tw_p));
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      a[m] = lane0(q[m]);
+      b[m] = lane1(q[m]);
+    }
+  } else {
+    fft<false, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+    fft<false, P>(b, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  }
   const double c1 = 2.0 * I.p.Q * I.p.kappa * I.dt;  // den = 1 + c1 k2^2
   const double kxf = kunit * (double)kx;
   const double kH2 = (kunit * (double)H) * (kunit * (double)H);
@@ -658,7 +695,11 @@ __global__ void __launch_bounds__(kBlock) k_col_b(const InstDev* __restrict__ in
       const int ky = t + T * m;
       const double kyf = kunit * (double)(ky < H ? ky : ky - N);
       const double k2 = kxf * kxf + kyf * kyf;
-      const WR iden = (WR)(1.0 / (1.0 + c1 * k2 * k2));
+      WR iden;
+      if constexpr (kSplitMixed<SR, WR>)
+        iden = __frcp_rn((float)fma(c1 * k2, k2, 1.0));  // FP32 reciprocal of the stabiliser
+      else
+        iden = (WR)(1.0 / (1.0 + c1 * k2 * k2));
       const WR kyd = (ky == H) ? (WR)0 : (WR)kyf;
       const cpx<WR> div = times_i(cscale(a[m], kxd) + cscale(b[m], kyd));
       a[m] = cscale(div, iden * dtn);

@@ -14,9 +14,6 @@
 
 namespace esc {
 
-// the mixed precision: FP64 state transforms, FP32 flux transforms
-template <typename SR, typename WR>
-constexpr bool kSplitMixed = std::is_same<SR, double>::value && std::is_same<WR, float>::value;
 
 // Plans with every group inside a warp (T <= 32) and E <= 16 where possible.
 template <int N>
@@ -26,10 +23,10 @@ struct WarpPlan {
 #define ESC_WPLAN(n, e, ...) \
   template <>                \
   struct WarpPlan<n> { using type = Plan<n, e, Radices<__VA_ARGS__>>; };
-ESC_WPLAN(96, 12, 6, 4, 4)
-ESC_WPLAN(384, 12, 6, 4, 4, 4)
+ESC_WPLAN(96, 12, 4, 4, 6)
+ESC_WPLAN(384, 12, 4, 4, 4, 6)
 ESC_WPLAN(512, 16, 16, 16, 2)
-ESC_WPLAN(768, 24, 12, 8, 8)
+ESC_WPLAN(768, 24, 8, 8, 12)
 #undef ESC_WPLAN
 
 template <class P>
