@@ -62,6 +62,7 @@ ESC_ALTPLAN(128, 8, 4, 4, 8)
 ESC_ALTPLAN(256, 8, 4, 8, 8)
 ESC_ALTPLAN(384, 12, 4, 4, 4, 6)
 ESC_ALTPLAN(768, 12, 4, 4, 4, 12)
+ESC_ALTPLAN(512, 16, 16, 16, 2)
 ESC_ALTPLAN(1024, 8, 4, 4, 8, 8)
 #undef ESC_ALTPLAN
 
@@ -234,16 +235,16 @@ struct KS {
   }
   static void row_a_w(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
     if constexpr (warp_ok)
-      k_row_a_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kBlock, warp_smem(), st>>>(d, base, s);
+      k_row_a_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kWarpBlock, warp_smem(), st>>>(d, base, s);
   }
   // the mixed precision transforms two rows per group in packed FP32 pairs
   static constexpr bool kPackedRows = std::is_same<SR, double>::value && std::is_same<WR, float>::value;
   static void row_b_w(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
     if constexpr (warp_ok) {
       if constexpr (kPackedRows)
-        k_row_b_w2<WP><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kBlock, warp_smem(), st>>>(d, base, s);
+        k_row_b_w2<WP><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kWarpBlock, warp_smem(), st>>>(d, base, s);
       else
-        k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kBlock, warp_smem(), st>>>(d, base, s);
+        k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kWarpBlock, warp_smem(), st>>>(d, base, s);
     }
   }
   // ---- alternative column plan ----
@@ -314,7 +315,7 @@ struct KS {
       const int alt_need = 5 * ((H + kBlock / AP::T - 1) / (kBlock / AP::T)) + alt_tiles_cols +
                            (N + kBlock / AP::T - 1) / (kBlock / AP::T);
       if (alt_need > need) need = alt_need;
-      const int wa = 5 * warp_tiles_pairs() * (kBlock / 32), wb = warp_tiles_rows() * (kBlock / 32);
+      const int wa = 5 * warp_tiles_pairs() * (kWarpBlock / 32), wb = warp_tiles_rows() * (kWarpBlock / 32);
       if (wa > need) need = wa;
       if (wb > need) need = wb;
       k.part_len = need;

@@ -29,12 +29,21 @@ ESC_WPLAN(512, 16, 16, 16, 2)
 ESC_WPLAN(768, 24, 8, 8, 12)
 #undef ESC_WPLAN
 
+// Blocks of the warp-independent kernels: no block-wide barrier ties their
+// warps together, so small blocks let every warp start as soon as one retires
+// and keep the warps of an SM spread over load and compute phases.
+#ifndef ESC_WARP_BLOCK
+#define ESC_WARP_BLOCK 32
+#endif
+constexpr int kWarpBlock = ESC_WARP_BLOCK;
+constexpr int kWarpBlocksPerSM = 512 / kWarpBlock;  // 16 warps per SM at up to 128 registers
+
 template <class P>
 struct WarpRowGeom {
   static constexpr int N = P::N, T = P::T, H = N / 2;
   static_assert(T <= 32 && 32 % T == 0, "warp kernels need groups inside one warp");
   static constexpr int GPW = 32 / T;            // groups per warp
-  static constexpr int NW = kBlock / 32;        // warps per block
+  static constexpr int NW = kWarpBlock / 32;    // warps per block
   static constexpr int G = GPW * NW;            // groups per block
   static constexpr int tiles_pairs = (H + G - 1) / G;
   static constexpr int tiles_rows = (N + G - 1) / G;
@@ -91,7 +100,7 @@ __device__ __forceinline__ bool warp_instance_running(const int* status) {
 
 // =====================================================================================
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kBlock, 2) k_row_a_w(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_a_w(const InstDev* __restrict__ insts,
                                                        const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
@@ -226,7 +235,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_row_a_w(const InstDev* __restrict
 
 // =====================================================================================
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kBlock, 2) k_row_b_w(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w(const InstDev* __restrict__ insts,
                                                        const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
@@ -334,7 +343,7 @@ __device__ __forceinline__ void split_rows_packed(const cpx<f2> (&y)[P::E], int 
 }
 
 template <class P>
-__global__ void __launch_bounds__(kBlock, 2) k_row_b_w2(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w2(const InstDev* __restrict__ insts,
                                                         const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
