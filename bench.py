@@ -14,6 +14,12 @@ is one time step of every particle (history row + stabilised update).
   adjoint gradient of 1/2|c_T - c_target|^2 + 1e-3 F[c_T] w.r.t. c0 and (P, chi, kappa, M0)
           through 2000 mixed-precision steps at 256^2 and 512^2 (checkpoints every 45):
           the reverse sweep (recompute + adjoint) per step over the forward step
+  large_grids  the single-grid configurations (1024^2 and 4096^2, 10,000 steps): FP64
+          drop-in and mixed rates side by side and the mixed error against FP64
+  accuracy  after 2000 steps of the ensemble: mixed precision against the FP64
+          drop-in per instance (max and L2 error of c, energy, mass drift), beside
+          the FP64 drop-in restarted from c0 perturbed by 1e-8 relative, which
+          measures how strongly the dynamics amplify any perturbation
 
 The working set (1.7 GB mixed, 2.6 GB FP64) is far larger than the 126 MB L2,
 so no flush is needed between steps.  Under torchrun every rank runs its own
@@ -191,6 +197,98 @@ def run_reference(args, world, rank):
     return 0
 
 
+def error_stats(cs, hs, ref_cs, ref_hs):
+    """Per-instance errors of fields cs / histories hs against the reference run."""
+    e_max = np.array([np.max(np.abs(a - b)) / np.max(np.abs(b)) for a, b in zip(cs, ref_cs)])
+    e_l2 = np.array([np.linalg.norm(a - b) / np.linalg.norm(b) for a, b in zip(cs, ref_cs)])
+    e_F = np.array([np.max(np.abs(h[2] - r[2]) / np.abs(r[2])) for h, r in zip(hs, ref_hs)])
+    mass = np.array([np.max(np.abs(h[1] - h[1][0])) for h in hs])
+    return {"max_rel_err_c": float(e_max.max()), "p50_max_rel_err_c": float(np.median(e_max)),
+            "p90_max_rel_err_c": float(np.quantile(e_max, 0.9)),
+            "frac_instances_le_1e-5": float(np.mean(e_max <= 1e-5)),
+            "l2_rel_err_c_max": float(e_l2.max()), "energy_rel_err_max": float(e_F.max()),
+            "mass_drift_max": float(mass.max())}
+
+
+def accuracy_block(phis, ps, c0s, steps):
+    """Mixed precision against the FP64 drop-in over the whole ensemble after
+    `steps` steps (the configuration's 2000), next to the FP64 drop-in started
+    from c0 perturbed by 1e-8 relative: spinodal decomposition amplifies any
+    perturbation, and the second row shows how far a 1e-8 change of the input
+    alone moves c (the conditioning of the problem, not an arithmetic error)."""
+    import torch
+    import esc
+
+    def run(prec, cs0):
+        b = esc.Batch(phis, params=ps, precision=prec)
+        work = [torch.from_numpy(c).cuda() for c in cs0]
+        hist = torch.zeros(len(cs0) * (steps + 1) * 6, dtype=torch.float64, device="cuda")
+        b.run_device([w.data_ptr() for w in work], steps, DT, hist.data_ptr())
+        torch.cuda.synchronize()
+        out = [w.cpu().numpy() for w in work]
+        h = hist.cpu().numpy().reshape(len(cs0), 6, steps + 1)
+        b.close()
+        return out, h
+
+    ref_c, ref_h = run("fp64", c0s)
+    mix_c, mix_h = run("mixed", c0s)
+    rng = np.random.default_rng(12345)
+    pert = [c * (1.0 + 1e-8 * (2.0 * rng.random(c.shape) - 1.0)) for c in c0s]
+    per_c, per_h = run("fp64", pert)
+    return {"steps": steps, "instances": len(c0s),
+            "mixed_vs_fp64": error_stats(mix_c, mix_h, ref_c, ref_h),
+            "fp64_from_c0_perturbed_1e-8_vs_fp64": error_stats(per_c, per_h, ref_c, ref_h),
+            "fp64_mass_drift_max": float(max(np.max(np.abs(h[1] - h[1][0])) for h in ref_h))}
+
+
+def single_grid_block(name, phi, c0, steps, peak_gbs):
+    """One large grid through the single-particle context: the FP64 drop-in and
+    the mixed precision side by side (device-resident, CUDA-event timed), with
+    the mixed result's error against the FP64 one (c, energy, mass drift)."""
+    import torch
+    import esc
+    n = phi.shape[0]
+    stream = torch.cuda.current_stream()
+    rates, out = {}, {}
+    for prec in ("fp64", "mixed"):
+        with esc.Context(phi, precision=prec) as ctx:
+            ctx.set_stream(stream.cuda_stream)
+            d = torch.from_numpy(c0).cuda()
+            h = torch.zeros(6 * (steps + 1), dtype=torch.float64, device="cuda")
+            ctx.run_device(d.data_ptr(), 3, DT)
+            d.copy_(torch.from_numpy(c0))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.run_device(d.data_ptr(), steps, DT, h.data_ptr())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            rates[prec] = n * n * steps / (e0.elapsed_time(e1) / 1000.0)
+            out[prec] = (d.cpu().numpy(), h.cpu().numpy().reshape(6, steps + 1))
+    err = error_stats([out["mixed"][0]], [out["mixed"][1]], [out["fp64"][0]], [out["fp64"][1]])
+    err.pop("p50_max_rel_err_c")
+    err.pop("p90_max_rel_err_c")
+    return {"config": name, "n": n, "steps": steps, "fp64_pt_steps_per_s": rates["fp64"],
+            "mixed_pt_steps_per_s": rates["mixed"], "mixed_over_fp64": rates["mixed"] / rates["fp64"],
+            "mixed_step_frac_of_hbm_roofline": rates["mixed"] * B_ALG_PER_STEP / (peak_gbs * 1e9),
+            "mixed_vs_fp64": err,
+            "fp64_mass_drift": float(np.max(np.abs(out["fp64"][1][1] - out["fp64"][1][1][0])))}
+
+
+def large_grid_configs(peak_gbs):
+    """The two single-grid configurations: 1024^2 disc (R = 400, w = 2, c0 = 0.5 +
+    U(-0.01, 0.01) over the whole field, seed 1) and the 4096^2 ellipse (semi-axes
+    1600 along x and 1200 along y, w = 2, c0 = 0.5 + mean-free U(-0.01, 0.01)
+    inside the particle, seed 5), 10,000 steps each, dt = 0.01."""
+    from esc import fields
+    phi2 = fields.particle_disc(1024, radius=400.0, width=2.0)
+    c02 = fields.whole_field_noise(1024, seed=1)
+    phi5 = fields.particle_ellipse(4096, a=1600.0, b=1200.0, width=2.0)
+    c05 = fields.interior_noise(phi5, 5)
+    return [single_grid_block("1024^2 disc R=400, 10000 steps", phi2, c02, 10000, peak_gbs),
+            single_grid_block("4096^2 ellipse 1600x1200, 10000 steps", phi5, c05, 10000, peak_gbs)]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -198,9 +296,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--count", type=int, default=COUNT)
+    ap.add_argument("--sizes", default=",".join(str(n) for n in SIZES),
+                    help="grid sizes the particles are drawn from (a single size gives a uniform batch, "
+                         "e.g. a small case for profiling)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=2000)
+    ap.add_argument("--no-large", action="store_true", help="skip the 1024^2 and 4096^2 single-grid runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -232,7 +336,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    ns, phis, c0s, ps = ensemble(count=args.count, seed_base=rank * args.count, rng_seed=rank)
+    sizes = tuple(int(x) for x in args.sizes.split(","))
+    ns, phis, c0s, ps = ensemble(count=args.count, seed_base=rank * args.count, rng_seed=rank, sizes=sizes)
     pts = sum(n * n for n in ns)
     dc0 = [torch.from_numpy(c).cuda() for c in c0s]
 
@@ -359,6 +464,13 @@ def main():
                             "adjoint_call_over_forward": ta / tf,
                             "dL_dtheta": [float(x) for x in th]})
 
+    accuracy = None
+    if not args.no_accuracy:
+        accuracy = accuracy_block(phis, ps, c0s, args.accuracy_steps)
+    large = None
+    if not args.no_large:
+        large = large_grid_configs(peak)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         idx = sample_subset(ns)
@@ -379,11 +491,12 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 state / f32 flux transforms",
         "data": "synthetic",
-        "config": {"workload": f"batched ensemble: {args.count} particles per GPU, n in {list(SIZES)}, "
+        "config": {"workload": f"batched ensemble: {args.count} particles per GPU, n in {list(sizes)}, "
                                f"{pts} points, dt=0.01, mixed precision",
                    "global_batch": args.count * world, "l2": "working set 1.7 GB >> 126 MB L2; no flush"},
         "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
-        "fp64_dropin": fp64, "max_abs_err_vs_fp64": max_err, "clocks": clocks,
+        "fp64_dropin": fp64, "max_abs_err_vs_fp64": max_err, "accuracy": accuracy, "large_grids": large,
+        "clocks": clocks,
         "adjoint": adjoint,
         "nonfinite_instances": int(sum(1 for x in bads if x >= 0)),
         "kernel_families": tuned,
