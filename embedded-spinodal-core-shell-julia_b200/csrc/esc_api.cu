@@ -132,6 +132,16 @@ int row_family_override() {
   return -1;
 }
 
+// ESC_COLS = block | pipe | alt forces one column-kernel family (measurement aid)
+int col_family_override() {
+  const char* v = getenv("ESC_COLS");
+  if (!v) return -1;
+  if (!strcmp(v, "block")) return 0;
+  if (!strcmp(v, "pipe")) return 1;
+  if (!strcmp(v, "alt")) return 2;
+  return -1;
+}
+
 struct Engine {
   int count = 0;
   int prec = 0;
@@ -528,7 +538,7 @@ esc_status autotune(Engine& E) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  const int reps = 3;
+  const int reps = 5;
   auto time_it = [&](auto&& launch) -> float {
     launch();  // warm-up
     cudaEventRecord(e0, st);
@@ -545,7 +555,10 @@ esc_status autotune(Engine& E) {
     // columns first (they leave F/G in place for the rows)
     float best_c = 1e30f;
     int best_cf = 0;
+    const int cfo = col_family_override();
     for (int cf = 0; cf < 3; ++cf) {
+      if (cfo >= 0 && cf != cfo && !(cf == 0 && ((cfo == 1 && !can_pipe_cols) || (cfo == 2 && g.ks->E_alt == g.ks->E))))
+        continue;
       if (cf == 1 && !can_pipe_cols) continue;
       if (cf == 2 && g.ks->E_alt == g.ks->E) continue;  // same plan as family 0
       g.pipe_cols = cf == 1;
