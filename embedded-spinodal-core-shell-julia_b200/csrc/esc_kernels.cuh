@@ -259,6 +259,13 @@ struct ColGeom {
   static constexpr int T = P::T;
   static constexpr int W = kBlock / T;
 };
+// Resident blocks per SM the column kernels are compiled for: the mixed
+// precision's transforms fit 3 blocks at up to 8 elements per thread and 2 at
+// up to 16; larger plans (and the FP64 drop-in) keep the compiler's choice.
+template <class P, typename SR, typename WR>
+constexpr int col_min_blocks() {
+  return kSplitMixed<SR, WR> ? (P::E <= 8 ? 3 : (P::E <= 16 ? 2 : 1)) : 1;
+}
 
 // init: c (FP64 real) -> S (packed x-transform), one row pair per group
 template <class P, typename SR>
@@ -424,7 +431,7 @@ __global__ void __launch_bounds__(kBlock) k_row_a(const InstDev* __restrict__ in
 
 // col A: y-FFT of S and F, gradient energy, mu^, inverse y-FFT of i k mu^ -> G
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kBlock) k_col_a(const InstDev* __restrict__ insts, const int* __restrict__ base,
+__global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a(const InstDev* __restrict__ insts, const int* __restrict__ base,
                                                   int s_local) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -617,7 +624,7 @@ __global__ void __launch_bounds__(kBlock) k_row_b(const InstDev* __restrict__ in
 
 // col B: y-FFT of the fluxes, divergence, stabilised increment, inverse y-FFT, S += increment
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kBlock) k_col_b(const InstDev* __restrict__ insts) {
+__global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b(const InstDev* __restrict__ insts) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];
