@@ -169,7 +169,7 @@ struct Engine {
     const esc::KernelSet* ks64 = nullptr;
     double *phi64 = nullptr, *target = nullptr, *part = nullptr, *scal = nullptr, *hist = nullptr,
            *acc = nullptr, *cout = nullptr;
-    double2 *F64 = nullptr, *Lam = nullptr, *Xg = nullptr, *ckpt = nullptr, *seg = nullptr;
+    double2 *F64 = nullptr, *Lam = nullptr, *Xg = nullptr, *ckpt = nullptr;
     esc::cpx2<double>* G64 = nullptr;
     void* tw64 = nullptr;
     unsigned *cnt = nullptr, *acnt = nullptr;
@@ -178,7 +178,11 @@ struct Engine {
     esc::InstDev* d_seed = nullptr;  // FP64 shadow instance with a 1-row history
     esc::InstDev* d_bwd = nullptr;   // FP64 shadow instance without history
     esc::InstDev* d_out = nullptr;   // final transform of the adjoint
-    esc::AdjDev* d_adj = nullptr;    // one per step of a segment
+    esc::AdjDev* d_adj = nullptr;    // one per step of a segment, per segment buffer
+    double2* seg_buf[2] = {nullptr, nullptr};  // recomputed states of a segment (double-buffered)
+    cudaStream_t sweep = nullptr;    // the adjoint sweep runs here, beside the next recompute
+    cudaEvent_t recomputed[2] = {nullptr, nullptr}, swept[2] = {nullptr, nullptr};
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (kind * 2 + buffer, steps) -> graph
   } adj;
 
   esc_status fail(esc_status s, const std::string& msg) {
@@ -205,6 +209,15 @@ struct Engine {
   void release() {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
+    for (auto& kv : adj.graphs) cudaGraphExecDestroy(kv.second);
+    adj.graphs.clear();
+    for (int b = 0; b < 2; ++b) {
+      if (adj.recomputed[b]) cudaEventDestroy(adj.recomputed[b]);
+      if (adj.swept[b]) cudaEventDestroy(adj.swept[b]);
+      adj.recomputed[b] = adj.swept[b] = nullptr;
+    }
+    if (adj.sweep) cudaStreamDestroy(adj.sweep);
+    adj.sweep = nullptr;
     for (cudaStream_t s : side) cudaStreamDestroy(s);
     side.clear();
     for (cudaEvent_t e : side_ev) cudaEventDestroy(e);
@@ -806,6 +819,36 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
 // checkpoint every `K` steps; backward pass recomputes each segment (storing its
 // states) and applies the FP64 adjoint step (esc_adjoint.cuh) from the last step
 // to the first.
+// Captures the launches `issue(stream)` makes as a CUDA graph, once per
+// (kind, segment buffer, steps), and returns the cached executable.  Kinds:
+// 0 forward steps, 1 recompute of a segment into a segment buffer, 2 adjoint
+// sweep over a segment buffer.
+template <class Issue>
+esc_status adjoint_graph(Engine& E, int kind, int buf, int len, cudaGraphExec_t* out, Issue&& issue) {
+  auto& A = E.adj;
+  const auto key = std::make_pair(kind * 2 + buf, len);
+  const auto it = A.graphs.find(key);
+  if (it != A.graphs.end()) {
+    *out = it->second;
+    return ESC_OK;
+  }
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(E.own, cudaStreamCaptureModeThreadLocal));
+  issue(E.own);
+  const cudaError_t ec = cudaStreamEndCapture(E.own, &graph);
+  if (ec != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return E.fail_cuda("cudaStreamEndCapture", ec);
+  }
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ex, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) return E.fail_cuda("cudaGraphInstantiate", ei);
+  A.graphs[key] = ex;
+  *out = ex;
+  return ESC_OK;
+}
+
 esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, const double* c_target, double lamF,
                           int K, double* dL_dc0, double* dL_dparams, double* Lout) {
   if (E.count != 1) return E.fail(ESC_EINVAL, "esc_adjoint needs a single-particle context");
@@ -864,9 +907,26 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
     A.ckpt_cap = nck;
   }
   if (K + 1 > A.seg_cap) {
-    TRY(E.alloc(&A.seg, (size_t)(K + 1) * H * n * 16, "adjoint segment"));
-    TRY(E.alloc(&A.d_adj, (size_t)K * sizeof(esc::AdjDev), "adjoint step descriptors"));
+    // the cached graphs of kinds 1 and 2 address the old segment buffers and descriptors
+    for (auto it = A.graphs.begin(); it != A.graphs.end();) {
+      if (it->first.first >= 2) {
+        cudaGraphExecDestroy(it->second);
+        it = A.graphs.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    TRY(E.alloc(&A.seg_buf[0], (size_t)(K + 1) * H * n * 16, "adjoint segment"));
+    TRY(E.alloc(&A.seg_buf[1], (size_t)(K + 1) * H * n * 16, "adjoint segment"));
+    TRY(E.alloc(&A.d_adj, (size_t)2 * K * sizeof(esc::AdjDev), "adjoint step descriptors"));
     A.seg_cap = K + 1;
+  }
+  if (!A.sweep) {
+    CK(cudaStreamCreateWithFlags(&A.sweep, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      CK(cudaEventCreateWithFlags(&A.recomputed[b], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&A.swept[b], cudaEventDisableTiming));
+    }
   }
   const size_t sbytes = (size_t)H * n * 16;
   double2* S = static_cast<double2*>(g.S);
@@ -883,9 +943,14 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
   CK(cudaMemsetAsync(g.cnt, 0, 4 * sizeof(unsigned), st));
   CK(cudaMemsetAsync(E.base, 0, sizeof(int), st));
   g.ks->init(g.d_inst, 1, st);
-  for (int s = 0; s < steps; ++s) {
-    if (s % K == 0) CK(cudaMemcpyAsync(A.ckpt + (size_t)(s / K) * H * n, S, sbytes, cudaMemcpyDeviceToDevice, st));
-    launch_step(E, 0, st);
+  for (int c = 0; c < nck; ++c) {
+    const int len = std::min(steps, (c + 1) * K) - c * K;
+    CK(cudaMemcpyAsync(A.ckpt + (size_t)c * H * n, S, sbytes, cudaMemcpyDeviceToDevice, st));
+    cudaGraphExec_t gx = nullptr;
+    TRY(adjoint_graph(E, 0, 0, len, &gx, [&](cudaStream_t cs) {
+      for (int j = 0; j < len; ++j) launch_step(E, 0, cs);
+    }));
+    CK(cudaGraphLaunch(gx, st));
   }
   CK(cudaGetLastError());
   // ---- seed: energy, mu and lam_T at the final field ----
@@ -951,30 +1016,58 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
   CK(cudaMemcpyAsync(&scal0, A.scal, sizeof scal0, cudaMemcpyDeviceToHost, st));
   CK(cudaGetLastError());
   // ---- backward over segments ----
-  std::vector<esc::AdjDev> steps_desc((size_t)K);
-  for (int seg = nck - 1; seg >= 0; --seg) {
-    const int s0 = seg * K, s1 = std::min(steps, s0 + K), len = s1 - s0;
+  // Segment buffers alternate: while the sweep stream runs the adjoint over
+  // segment k (reading its buffer), the context stream recomputes segment k-1
+  // into the other buffer.  The two touch disjoint memory: the recompute uses
+  // the forward state and scratch, the sweep the adjoint's own buffers.
+  std::vector<esc::AdjDev> steps_desc((size_t)2 * K);
+  for (int b = 0; b < 2; ++b)
+    for (int j = 0; j < K; ++j) {
+      esc::AdjDev& q = steps_desc[(size_t)b * K + j];
+      q = ad;
+      q.S0 = A.seg_buf[b] + (size_t)j * H * n;
+      q.S1 = A.seg_buf[b] + (size_t)(j + 1) * H * n;
+    }
+  CK(cudaMemcpyAsync(A.d_adj, steps_desc.data(), steps_desc.size() * sizeof(esc::AdjDev), cudaMemcpyHostToDevice,
+                     st));
+  auto seg_len = [&](int seg) { return std::min(steps, (seg + 1) * K) - seg * K; };
+  auto recompute = [&](int seg, int b) -> esc_status {
+    const int len = seg_len(seg);
     const double2* ck = A.ckpt + (size_t)seg * H * n;
-    CK(cudaMemcpyAsync(A.seg, ck, sbytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamWaitEvent(st, A.swept[b], 0));  // the sweep that last read this buffer is done
+    CK(cudaMemcpyAsync(A.seg_buf[b], ck, sbytes, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(S, ck, sbytes, cudaMemcpyDeviceToDevice, st));
-    for (int j = 1; j <= len; ++j) {
-      launch_step(E, 0, st);
-      CK(cudaMemcpyAsync(A.seg + (size_t)j * H * n, S, sbytes, cudaMemcpyDeviceToDevice, st));
-    }
-    for (int j = 0; j < len; ++j) {
-      steps_desc[j] = ad;
-      steps_desc[j].S0 = A.seg + (size_t)j * H * n;
-      steps_desc[j].S1 = A.seg + (size_t)(j + 1) * H * n;
-    }
-    CK(cudaMemcpyAsync(A.d_adj, steps_desc.data(), (size_t)len * sizeof(esc::AdjDev), cudaMemcpyHostToDevice, st));
-    for (int j = len - 1; j >= 0; --j) {
-      k64->adj_col1(A.d_adj + j, 1, st);
-      k64->row_b(A.d_bwd, 1, A.zero, 0, st);
-      k64->adj_col2(A.d_adj + j, 1, st);
-      k64->adj_row2(A.d_adj + j, 1, st);
-    }
-    // the descriptors of this segment must not be overwritten before its kernels ran
-    CK(cudaStreamSynchronize(st));
+    cudaGraphExec_t gx = nullptr;
+    TRY(adjoint_graph(E, 1, b, len, &gx, [&](cudaStream_t cs) {
+      for (int j = 1; j <= len; ++j) {
+        launch_step(E, 0, cs);
+        cudaMemcpyAsync(A.seg_buf[b] + (size_t)j * H * n, S, sbytes, cudaMemcpyDeviceToDevice, cs);
+      }
+    }));
+    CK(cudaGraphLaunch(gx, st));
+    CK(cudaEventRecord(A.recomputed[b], st));
+    return ESC_OK;
+  };
+  int b = 0;
+  TRY(recompute(nck - 1, b));
+  for (int seg = nck - 1; seg >= 0; --seg) {
+    const int len = seg_len(seg);
+    CK(cudaStreamWaitEvent(A.sweep, A.recomputed[b], 0));
+    cudaGraphExec_t gx = nullptr;
+    esc::AdjDev* dd = A.d_adj + (size_t)b * K;
+    TRY(adjoint_graph(E, 2, b, len, &gx, [&](cudaStream_t cs) {
+      for (int j = len - 1; j >= 0; --j) {
+        k64->adj_col1(dd + j, 1, cs);
+        k64->row_b(A.d_bwd, 1, A.zero, 0, cs);
+        k64->adj_col2(dd + j, 1, cs);
+        k64->adj_row2(dd + j, 1, cs);
+      }
+    }));
+    CK(cudaGraphLaunch(gx, A.sweep));
+    CK(cudaEventRecord(A.swept[b], A.sweep));
+    if (seg > 0) TRY(recompute(seg - 1, 1 - b));
+    if (seg == 0) CK(cudaStreamWaitEvent(st, A.swept[b], 0));
+    b = 1 - b;
   }
   CK(cudaGetLastError());
   k64->fin(A.d_out, 1, st);
