@@ -14,6 +14,8 @@ is one time step of every particle (history row + stabilised update).
   adjoint gradient of 1/2|c_T - c_target|^2 + 1e-3 F[c_T] w.r.t. c0 and (P, chi, kappa, M0)
           through 2000 mixed-precision steps at 256^2 and 512^2 (checkpoints every 45):
           the reverse sweep (recompute + adjoint) per step over the forward step
+  batched_gradients  64 particles at 512^2, dL/d(P, chi, kappa, M0) through 1000 steps in
+          one esc_batch_adjoint call: gradient throughput and cost against a forward run
   large_grids  the single-grid configurations (1024^2 and 4096^2, 10,000 steps): FP64
           drop-in and mixed rates side by side and the mixed error against FP64
   accuracy  after 2000 steps of the ensemble: mixed precision against the FP64
@@ -289,6 +291,36 @@ def large_grid_configs(peak_gbs):
             single_grid_block("4096^2 ellipse 1600x1200, 10000 steps", phi5, c05, 10000, peak_gbs)]
 
 
+def batched_gradient_block(count=64, n=512, steps=1000):
+    """Batched parameter-fit gradients: `count` particles at n^2 (disc R ~ U(0.25, 0.42) n,
+    w = 2, sampled P, chi, kappa as in the ensemble), loss 1/2 |c_T - c_target|^2 + 1e-3 F[c_T]
+    with c_target a forward run at (1.1 P, 0.9 chi), gradients w.r.t. (P, chi, kappa, M0)
+    through `steps` steps for all particles in one esc_batch_adjoint call (mixed-precision
+    forward and recompute, FP64 adjoint).  Reports the gradient throughput and its cost
+    against a forward run of the same batch."""
+    import esc
+    ns, phis, c0s, ps = ensemble(count=count, seed_base=1000, sizes=(n,), rng_seed=7)
+    pts = [esc.Parameters(A=p.A, B=p.B, chi=p.chi * 0.9, P=p.P * 1.1, ca=p.ca, cb=p.cb, cc=p.cc,
+                          kappa=p.kappa, mobility=p.mobility, Q=p.Q) for p in ps]
+    with esc.Batch(phis, params=pts, precision="mixed") as bt:
+        targets, _, _ = bt.run(c0s, dt=DT, steps=steps, with_history=False)
+    with esc.Batch(phis, params=ps, precision="mixed") as b:
+        # warm-up with the timed shapes: the step graphs of a gradient call are built once per
+        # (segment length, buffer) and reused, as in the repeated calls of a parameter fit
+        b.run(c0s, dt=DT, steps=steps, with_history=False)
+        b.adjoint(c0s, targets, dt=DT, steps=steps, lambda_F=1e-3, with_field_gradients=False)
+        t0 = time.perf_counter()
+        b.run(c0s, dt=DT, steps=steps, with_history=False)
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        L, _, th = b.adjoint(c0s, targets, dt=DT, steps=steps, lambda_F=1e-3, with_field_gradients=False)
+        t_adj = time.perf_counter() - t0
+    return {"particles": count, "n": n, "steps": steps, "gradient_call_s": t_adj, "forward_call_s": t_fwd,
+            "gradient_pt_steps_per_s": count * n * n * steps / t_adj,
+            "gradient_call_over_forward_call": t_adj / t_fwd,
+            "dL_dtheta_particle0": [float(x) for x in th[0]], "L_particle0": float(L[0])}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -451,7 +483,7 @@ def main():
             ct, _ = esc.run_simulation(c0, phi, dt=DT, steps=2000, p=pt, precision="mixed")
             with esc.Context(phi, precision="mixed") as ctx:
                 ctx.run(c0, dt=DT, steps=20, with_history=False)
-                ctx.adjoint(c0, ct, dt=DT, steps=20, lambda_F=1e-3, ckpt_every=5)
+                ctx.adjoint(c0, ct, dt=DT, steps=2000, lambda_F=1e-3, ckpt_every=45)  # builds the step graphs
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 ctx.run(c0, dt=DT, steps=2000, with_history=False)
@@ -470,6 +502,9 @@ def main():
     large = None
     if not args.no_large:
         large = large_grid_configs(peak)
+    batched_grad = None
+    if not args.no_adjoint:
+        batched_grad = batched_gradient_block()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -497,7 +532,7 @@ def main():
         "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
         "fp64_dropin": fp64, "max_abs_err_vs_fp64": max_err, "accuracy": accuracy, "large_grids": large,
         "clocks": clocks,
-        "adjoint": adjoint,
+        "adjoint": adjoint, "batched_gradients": batched_grad,
         "nonfinite_instances": int(sum(1 for x in bads if x >= 0)),
         "kernel_families": tuned,
     }

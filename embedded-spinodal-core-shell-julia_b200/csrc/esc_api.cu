@@ -183,6 +183,7 @@ struct Engine {
     cudaStream_t sweep = nullptr;    // the adjoint sweep runs here, beside the next recompute
     cudaEvent_t recomputed[2] = {nullptr, nullptr}, swept[2] = {nullptr, nullptr};
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (kind * 2 + buffer, steps) -> graph
+    size_t pstride = 0;              // partial-sum doubles per instance
   } adj;
 
   esc_status fail(esc_status s, const std::string& msg) {
@@ -849,17 +850,21 @@ esc_status adjoint_graph(Engine& E, int kind, int buf, int len, cudaGraphExec_t*
   return ESC_OK;
 }
 
-esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, const double* c_target, double lamF,
-                          int K, double* dL_dc0, double* dL_dparams, double* Lout) {
-  if (E.count != 1) return E.fail(ESC_EINVAL, "esc_adjoint needs a single-particle context");
+esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double dt, const double* const* c_target,
+                          double lamF, int K, double* const* dL_dc0, double* dL_dparams, double* Lout) {
+  if (E.groups.size() != 1) return E.fail(ESC_EINVAL, "the adjoint needs all particles of one grid size");
   if (steps < 1 || !c0 || !c_target) return E.fail(ESC_EINVAL, "bad adjoint arguments");
   if (!std::isfinite(dt) || !std::isfinite(lamF)) return E.fail(ESC_EINVAL, "dt and lambda_F must be finite");
+  Group& g = E.groups[0];
+  const int cnt = (int)g.members.size();
+  for (int s = 0; s < cnt; ++s)
+    if (!c0[g.members[s]] || !c_target[g.members[s]]) return E.fail(ESC_EINVAL, "null field in the adjoint inputs");
   if (K < 1) K = (int)std::ceil(std::sqrt((double)steps));
   if (K > steps) K = steps;
   DeviceGuard dg(E.device);
-  Group& g = E.groups[0];
   const int n = g.n, H = n / 2;
   const size_t nn = (size_t)n * n;
+  const size_t hn = (size_t)H * n;  // complex values of one instance's mixed-domain field
   auto& A = E.adj;
   cudaStream_t st = E.stream;
   const int nck = (steps + K - 1) / K;
@@ -868,42 +873,43 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
     if (!A.ks64 || !A.ks64->adj_col1) return E.fail(ESC_EINVAL, "no adjoint kernels for this size");
     CK(A.ks64->prepare());
     CK(A.ks64->prepare_adj());
-    TRY(E.alloc(&A.phi64, nn * 8, "adjoint phi"));
-    TRY(E.alloc(&A.target, nn * 8, "adjoint target"));
-    TRY(E.alloc(&A.cout, nn * 8, "adjoint output"));
-    TRY(E.alloc(&A.F64, (size_t)H * n * 16, "adjoint F"));
-    TRY(E.alloc(&A.Lam, (size_t)H * n * 16, "adjoint state"));
-    TRY(E.alloc(&A.Xg, (size_t)H * n * 16, "adjoint Xg"));
-    TRY(E.alloc(&A.G64, (size_t)H * n * 32, "adjoint G"));
+    A.pstride = (size_t)A.ks64->part_len + 8 * 4096;
+    TRY(E.alloc(&A.phi64, cnt * nn * 8, "adjoint phi"));
+    TRY(E.alloc(&A.target, cnt * nn * 8, "adjoint target"));
+    TRY(E.alloc(&A.cout, cnt * nn * 8, "adjoint output"));
+    TRY(E.alloc(&A.F64, cnt * hn * 16, "adjoint F"));
+    TRY(E.alloc(&A.Lam, cnt * hn * 16, "adjoint state"));
+    TRY(E.alloc(&A.Xg, cnt * hn * 16, "adjoint Xg"));
+    TRY(E.alloc(&A.G64, cnt * hn * 32, "adjoint G"));
     TRY(E.alloc(&A.tw64, (size_t)n * 16, "adjoint twiddles"));
-    TRY(E.alloc(&A.part, (size_t)(A.ks64->part_len + 8 * 4096) * 8, "adjoint partials"));
-    TRY(E.alloc(&A.scal, 64, "adjoint scalars"));
-    TRY(E.alloc(&A.hist, 6 * 8, "adjoint history row"));
-    TRY(E.alloc(&A.acc, 8 * 8, "adjoint accumulators"));
-    TRY(E.alloc(&A.cnt, 4 * 4, "adjoint counters"));
-    TRY(E.alloc(&A.acnt, 4 * 4, "adjoint counters"));
-    TRY(E.alloc(&A.status, 4, "adjoint status"));
+    TRY(E.alloc(&A.part, cnt * A.pstride * 8, "adjoint partials"));
+    TRY(E.alloc(&A.scal, cnt * 8 * 8, "adjoint scalars"));
+    TRY(E.alloc(&A.hist, cnt * 6 * 8, "adjoint history row"));
+    TRY(E.alloc(&A.acc, cnt * 8 * 8, "adjoint accumulators"));
+    TRY(E.alloc(&A.cnt, cnt * 4 * 4, "adjoint counters"));
+    TRY(E.alloc(&A.acnt, cnt * 4 * 4, "adjoint counters"));
+    TRY(E.alloc(&A.status, cnt * 4, "adjoint status"));
     TRY(E.alloc(&A.zero, 4, "zero"));
-    TRY(E.alloc(&A.bad, 8, "adjoint bad step"));
-    TRY(E.alloc(&A.d_seed, sizeof(esc::InstDev), "adjoint descriptor"));
-    TRY(E.alloc(&A.d_bwd, sizeof(esc::InstDev), "adjoint descriptor"));
-    TRY(E.alloc(&A.d_out, sizeof(esc::InstDev), "adjoint descriptor"));
-    // FP64 particle field and twiddles
+    TRY(E.alloc(&A.bad, cnt * 8, "adjoint bad step"));
+    TRY(E.alloc(&A.d_seed, cnt * sizeof(esc::InstDev), "adjoint descriptor"));
+    TRY(E.alloc(&A.d_bwd, cnt * sizeof(esc::InstDev), "adjoint descriptor"));
+    TRY(E.alloc(&A.d_out, cnt * sizeof(esc::InstDev), "adjoint descriptor"));
+    // FP64 particle fields and twiddles
     if (g.ks->wr_bytes == 8) {
-      CK(cudaMemcpy(A.phi64, g.phi, nn * 8, cudaMemcpyDeviceToDevice));
+      CK(cudaMemcpy(A.phi64, g.phi, cnt * nn * 8, cudaMemcpyDeviceToDevice));
     } else {
-      std::vector<float> pf(nn);
-      std::vector<double> pd(nn);
-      CK(cudaMemcpy(pf.data(), g.phi, nn * 4, cudaMemcpyDeviceToHost));
-      for (size_t k = 0; k < nn; ++k) pd[k] = (double)pf[k];
-      CK(cudaMemcpy(A.phi64, pd.data(), nn * 8, cudaMemcpyHostToDevice));
+      std::vector<float> pf(cnt * nn);
+      std::vector<double> pd(cnt * nn);
+      CK(cudaMemcpy(pf.data(), g.phi, cnt * nn * 4, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < cnt * nn; ++k) pd[k] = (double)pf[k];
+      CK(cudaMemcpy(A.phi64, pd.data(), cnt * nn * 8, cudaMemcpyHostToDevice));
     }
     if (g.ks->sr_bytes == 8) CK(cudaMemcpy(A.tw64, g.tw_s, (size_t)n * 16, cudaMemcpyDeviceToDevice));
     CK(cudaMemset(A.zero, 0, 4));
     A.ready = true;
   }
   if (nck > A.ckpt_cap) {
-    TRY(E.alloc(&A.ckpt, (size_t)nck * H * n * 16, "adjoint checkpoints"));
+    TRY(E.alloc(&A.ckpt, (size_t)nck * cnt * hn * 16, "adjoint checkpoints"));
     A.ckpt_cap = nck;
   }
   if (K + 1 > A.seg_cap) {
@@ -916,9 +922,9 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
         ++it;
       }
     }
-    TRY(E.alloc(&A.seg_buf[0], (size_t)(K + 1) * H * n * 16, "adjoint segment"));
-    TRY(E.alloc(&A.seg_buf[1], (size_t)(K + 1) * H * n * 16, "adjoint segment"));
-    TRY(E.alloc(&A.d_adj, (size_t)2 * K * sizeof(esc::AdjDev), "adjoint step descriptors"));
+    TRY(E.alloc(&A.seg_buf[0], (size_t)(K + 1) * cnt * hn * 16, "adjoint segment"));
+    TRY(E.alloc(&A.seg_buf[1], (size_t)(K + 1) * cnt * hn * 16, "adjoint segment"));
+    TRY(E.alloc(&A.d_adj, (size_t)2 * K * cnt * sizeof(esc::AdjDev), "adjoint step descriptors"));
     A.seg_cap = K + 1;
   }
   if (!A.sweep) {
@@ -928,24 +934,26 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
       CK(cudaEventCreateWithFlags(&A.swept[b], cudaEventDisableTiming));
     }
   }
-  const size_t sbytes = (size_t)H * n * 16;
+  const size_t sbytes = (size_t)cnt * hn * 16;  // the whole group's state
   double2* S = static_cast<double2*>(g.S);
   // ---- forward pass with checkpoints ----
-  esc::InstDev& d = g.h_inst[0];
-  d.dt = dt;
-  d.hist = nullptr;
-  d.hist_ld = 1;
-  d.cio = g.cio;
-  CK(cudaMemcpyAsync(g.d_inst, &d, sizeof d, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(g.cio, c0, nn * 8, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(A.target, c_target, nn * 8, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(g.status, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(g.cnt, 0, 4 * sizeof(unsigned), st));
+  for (int s = 0; s < cnt; ++s) {
+    esc::InstDev& d = g.h_inst[s];
+    d.dt = dt;
+    d.hist = nullptr;
+    d.hist_ld = 1;
+    d.cio = g.cio + s * nn;
+    CK(cudaMemcpyAsync(g.cio + s * nn, c0[g.members[s]], nn * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(A.target + s * nn, c_target[g.members[s]], nn * 8, cudaMemcpyHostToDevice, st));
+  }
+  CK(cudaMemcpyAsync(g.d_inst, g.h_inst.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(g.status, 0, cnt * sizeof(int), st));
+  CK(cudaMemsetAsync(g.cnt, 0, cnt * 4 * sizeof(unsigned), st));
   CK(cudaMemsetAsync(E.base, 0, sizeof(int), st));
-  g.ks->init(g.d_inst, 1, st);
+  g.ks->init(g.d_inst, cnt, st);
   for (int c = 0; c < nck; ++c) {
     const int len = std::min(steps, (c + 1) * K) - c * K;
-    CK(cudaMemcpyAsync(A.ckpt + (size_t)c * H * n, S, sbytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(A.ckpt + (size_t)c * cnt * hn, S, sbytes, cudaMemcpyDeviceToDevice, st));
     cudaGraphExec_t gx = nullptr;
     TRY(adjoint_graph(E, 0, 0, len, &gx, [&](cudaStream_t cs) {
       for (int j = 0; j < len; ++j) launch_step(E, 0, cs);
@@ -953,87 +961,94 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
     CK(cudaGraphLaunch(gx, st));
   }
   CK(cudaGetLastError());
-  // ---- seed: energy, mu and lam_T at the final field ----
+  // ---- seed: energy, mu and lam_T at the final fields ----
   const esc::KernelSet* k64 = A.ks64;
-  esc::InstDev sd;
-  memset(&sd, 0, sizeof sd);
-  sd.n = n;
-  sd.hist_ld = 1;
-  sd.dx = g.h_inst[0].dx;
-  sd.dt = dt;
-  sd.p = g.h_inst[0].p;
-  sd.S = S;
-  sd.F = A.F64;
-  sd.G = A.G64;
-  sd.phi = A.phi64;
-  sd.hist = A.hist;
-  sd.part = A.part;
-  sd.cnt = A.cnt;
-  sd.scal = A.scal;
-  sd.status = A.status;
-  sd.bad_step = A.bad;
-  sd.tw_s = A.tw64;
-  sd.tw_w = A.tw64;
-  sd.cio = A.cout;
-  esc::InstDev bd = sd;
-  bd.hist = nullptr;
-  esc::InstDev od = sd;
-  od.S = A.Lam;
-  od.hist = nullptr;
-  CK(cudaMemcpyAsync(A.d_seed, &sd, sizeof sd, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(A.d_bwd, &bd, sizeof bd, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(A.d_out, &od, sizeof od, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(A.cnt, 0, 16, st));
-  CK(cudaMemsetAsync(A.acnt, 0, 16, st));
-  CK(cudaMemsetAsync(A.status, 0, 4, st));
-  CK(cudaMemsetAsync(A.acc, 0, 64, st));
-  k64->row_a(A.d_seed, 1, A.zero, 0, st);
-  k64->col_a(A.d_seed, 1, A.zero, 0, st);
-  esc::AdjDev ad;
-  memset(&ad, 0, sizeof ad);
-  ad.n = n;
-  ad.dx = sd.dx;
-  ad.dt = dt;
-  ad.lamF = lamF;
-  ad.p = sd.p;
-  ad.S0 = S;
-  ad.S1 = S;
-  ad.Lam = A.Lam;
-  ad.Xg = A.Xg;
-  ad.F = A.F64;
-  ad.G = A.G64;
-  ad.phi = A.phi64;
-  ad.target = A.target;
-  ad.tw = A.tw64;
-  ad.part = A.part;
-  ad.cnt = A.acnt;
-  ad.acc = A.acc;
-  CK(cudaMemcpyAsync(A.d_adj, &ad, sizeof ad, cudaMemcpyHostToDevice, st));
-  k64->adj_mu_col(A.d_adj, 1, st);
-  k64->adj_seed_row(A.d_adj, 1, st);
-  double hist_row[6], scal0 = 0.0;
-  CK(cudaMemcpyAsync(hist_row, A.hist, sizeof hist_row, cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(&scal0, A.scal, sizeof scal0, cudaMemcpyDeviceToHost, st));
+  std::vector<esc::InstDev> sd((size_t)cnt), bd((size_t)cnt), od((size_t)cnt);
+  std::vector<esc::AdjDev> ad((size_t)cnt);
+  for (int s = 0; s < cnt; ++s) {
+    esc::InstDev& q = sd[s];
+    memset(&q, 0, sizeof q);
+    q.n = n;
+    q.hist_ld = 1;
+    q.dx = g.h_inst[s].dx;
+    q.dt = dt;
+    q.p = g.h_inst[s].p;
+    q.S = S + s * hn;
+    q.F = A.F64 + s * hn;
+    q.G = A.G64 + s * hn;
+    q.phi = A.phi64 + s * nn;
+    q.hist = A.hist + 6 * s;
+    q.part = A.part + s * A.pstride;
+    q.cnt = A.cnt + 4 * s;
+    q.scal = A.scal + 8 * s;
+    q.status = A.status + s;
+    q.bad_step = A.bad + s;
+    q.tw_s = A.tw64;
+    q.tw_w = A.tw64;
+    q.cio = A.cout + s * nn;
+    bd[s] = q;
+    bd[s].hist = nullptr;
+    od[s] = q;
+    od[s].S = A.Lam + s * hn;
+    od[s].hist = nullptr;
+    esc::AdjDev& a = ad[s];
+    memset(&a, 0, sizeof a);
+    a.n = n;
+    a.dx = q.dx;
+    a.dt = dt;
+    a.lamF = lamF;
+    a.p = q.p;
+    a.S0 = S + s * hn;
+    a.S1 = S + s * hn;
+    a.Lam = A.Lam + s * hn;
+    a.Xg = A.Xg + s * hn;
+    a.F = A.F64 + s * hn;
+    a.G = A.G64 + s * hn;
+    a.phi = A.phi64 + s * nn;
+    a.target = A.target + s * nn;
+    a.tw = A.tw64;
+    a.part = A.part + s * A.pstride;
+    a.cnt = A.acnt + 4 * s;
+    a.acc = A.acc + 8 * s;
+  }
+  CK(cudaMemcpyAsync(A.d_seed, sd.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(A.d_bwd, bd.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(A.d_out, od.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(A.cnt, 0, cnt * 16, st));
+  CK(cudaMemsetAsync(A.acnt, 0, cnt * 16, st));
+  CK(cudaMemsetAsync(A.status, 0, cnt * 4, st));
+  CK(cudaMemsetAsync(A.acc, 0, cnt * 64, st));
+  k64->row_a(A.d_seed, cnt, A.zero, 0, st);
+  k64->col_a(A.d_seed, cnt, A.zero, 0, st);
+  CK(cudaMemcpyAsync(A.d_adj, ad.data(), cnt * sizeof(esc::AdjDev), cudaMemcpyHostToDevice, st));
+  k64->adj_mu_col(A.d_adj, cnt, st);
+  k64->adj_seed_row(A.d_adj, cnt, st);
+  std::vector<double> hist_rows((size_t)cnt * 6), scal((size_t)cnt * 8);
+  CK(cudaMemcpyAsync(hist_rows.data(), A.hist, cnt * 6 * 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(scal.data(), A.scal, cnt * 8 * 8, cudaMemcpyDeviceToHost, st));
   CK(cudaGetLastError());
   // ---- backward over segments ----
   // Segment buffers alternate: while the sweep stream runs the adjoint over
   // segment k (reading its buffer), the context stream recomputes segment k-1
   // into the other buffer.  The two touch disjoint memory: the recompute uses
   // the forward state and scratch, the sweep the adjoint's own buffers.
-  std::vector<esc::AdjDev> steps_desc((size_t)2 * K);
+  // Step j of buffer b, instance s: descriptor (b*K + j)*cnt + s, states at
+  // seg_buf[b] + (j*cnt + s)*hn and (j+1).
+  std::vector<esc::AdjDev> steps_desc((size_t)2 * K * cnt);
   for (int b = 0; b < 2; ++b)
-    for (int j = 0; j < K; ++j) {
-      esc::AdjDev& q = steps_desc[(size_t)b * K + j];
-      q = ad;
-      q.S0 = A.seg_buf[b] + (size_t)j * H * n;
-      q.S1 = A.seg_buf[b] + (size_t)(j + 1) * H * n;
-    }
+    for (int j = 0; j < K; ++j)
+      for (int s = 0; s < cnt; ++s) {
+        esc::AdjDev& q = steps_desc[((size_t)b * K + j) * cnt + s];
+        q = ad[s];
+        q.S0 = A.seg_buf[b] + ((size_t)j * cnt + s) * hn;
+        q.S1 = A.seg_buf[b] + ((size_t)(j + 1) * cnt + s) * hn;
+      }
   CK(cudaMemcpyAsync(A.d_adj, steps_desc.data(), steps_desc.size() * sizeof(esc::AdjDev), cudaMemcpyHostToDevice,
                      st));
   auto seg_len = [&](int seg) { return std::min(steps, (seg + 1) * K) - seg * K; };
   auto recompute = [&](int seg, int b) -> esc_status {
     const int len = seg_len(seg);
-    const double2* ck = A.ckpt + (size_t)seg * H * n;
+    const double2* ck = A.ckpt + (size_t)seg * cnt * hn;
     CK(cudaStreamWaitEvent(st, A.swept[b], 0));  // the sweep that last read this buffer is done
     CK(cudaMemcpyAsync(A.seg_buf[b], ck, sbytes, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(S, ck, sbytes, cudaMemcpyDeviceToDevice, st));
@@ -1041,7 +1056,7 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
     TRY(adjoint_graph(E, 1, b, len, &gx, [&](cudaStream_t cs) {
       for (int j = 1; j <= len; ++j) {
         launch_step(E, 0, cs);
-        cudaMemcpyAsync(A.seg_buf[b] + (size_t)j * H * n, S, sbytes, cudaMemcpyDeviceToDevice, cs);
+        cudaMemcpyAsync(A.seg_buf[b] + (size_t)j * cnt * hn, S, sbytes, cudaMemcpyDeviceToDevice, cs);
       }
     }));
     CK(cudaGraphLaunch(gx, st));
@@ -1054,13 +1069,13 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
     const int len = seg_len(seg);
     CK(cudaStreamWaitEvent(A.sweep, A.recomputed[b], 0));
     cudaGraphExec_t gx = nullptr;
-    esc::AdjDev* dd = A.d_adj + (size_t)b * K;
+    esc::AdjDev* dd = A.d_adj + (size_t)b * K * cnt;
     TRY(adjoint_graph(E, 2, b, len, &gx, [&](cudaStream_t cs) {
       for (int j = len - 1; j >= 0; --j) {
-        k64->adj_col1(dd + j, 1, cs);
-        k64->row_b(A.d_bwd, 1, A.zero, 0, cs);
-        k64->adj_col2(dd + j, 1, cs);
-        k64->adj_row2(dd + j, 1, cs);
+        k64->adj_col1(dd + (size_t)j * cnt, cnt, cs);
+        k64->row_b(A.d_bwd, cnt, A.zero, 0, cs);
+        k64->adj_col2(dd + (size_t)j * cnt, cnt, cs);
+        k64->adj_row2(dd + (size_t)j * cnt, cnt, cs);
       }
     }));
     CK(cudaGraphLaunch(gx, A.sweep));
@@ -1070,24 +1085,32 @@ esc_status engine_adjoint(Engine& E, const double* c0, int steps, double dt, con
     b = 1 - b;
   }
   CK(cudaGetLastError());
-  k64->fin(A.d_out, 1, st);
-  double acc[8];
-  CK(cudaMemcpyAsync(acc, A.acc, sizeof acc, cudaMemcpyDeviceToHost, st));
-  if (dL_dc0) CK(cudaMemcpyAsync(dL_dc0, A.cout, nn * 8, cudaMemcpyDeviceToHost, st));
-  int fstatus = 0;
-  CK(cudaMemcpyAsync(&fstatus, g.status, sizeof fstatus, cudaMemcpyDeviceToHost, st));
+  k64->fin(A.d_out, cnt, st);
+  std::vector<double> acc((size_t)cnt * 8);
+  CK(cudaMemcpyAsync(acc.data(), A.acc, cnt * 64, cudaMemcpyDeviceToHost, st));
+  for (int s = 0; s < cnt; ++s)
+    if (dL_dc0 && dL_dc0[g.members[s]])
+      CK(cudaMemcpyAsync(dL_dc0[g.members[s]], A.cout + s * nn, nn * 8, cudaMemcpyDeviceToHost, st));
+  std::vector<int> fstatus((size_t)cnt);
+  CK(cudaMemcpyAsync(fstatus.data(), g.status, cnt * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (fstatus) return E.fail(ESC_ENONFINITE, "Non-finite composition during the adjoint's forward pass");
-  const double dx2 = sd.dx * sd.dx;
-  const double E_T = hist_row[2];
-  const esc::ModelParams& p = sd.p;
-  if (dL_dparams) {
-    dL_dparams[0] = acc[0] + lamF * acc[5] * dx2;
-    dL_dparams[1] = acc[1] + lamF * (-p.P * acc[6] * dx2);
-    dL_dparams[2] = acc[2] + lamF * ((E_T - scal0 * dx2) / p.kappa);
-    dL_dparams[3] = acc[3];
+  for (int s = 0; s < cnt; ++s)
+    if (fstatus[s]) return E.fail(ESC_ENONFINITE, "Non-finite composition during the adjoint's forward pass");
+  for (int s = 0; s < cnt; ++s) {
+    const int i = g.members[s];
+    const double dx2 = sd[s].dx * sd[s].dx;
+    const double E_T = hist_rows[6 * s + 2];
+    const double scal0 = scal[8 * s];
+    const double* a = &acc[8 * s];
+    const esc::ModelParams& p = sd[s].p;
+    if (dL_dparams) {
+      dL_dparams[4 * i + 0] = a[0] + lamF * a[5] * dx2;
+      dL_dparams[4 * i + 1] = a[1] + lamF * (-p.P * a[6] * dx2);
+      dL_dparams[4 * i + 2] = a[2] + lamF * ((E_T - scal0 * dx2) / p.kappa);
+      dL_dparams[4 * i + 3] = a[3];
+    }
+    if (Lout) Lout[i] = a[4] + lamF * E_T;
   }
-  if (Lout) *Lout = acc[4] + lamF * E_T;
   return ESC_OK;
 }
 
@@ -1308,7 +1331,20 @@ esc_status esc_adjoint(esc_ctx* ctx, const double* c0, int steps, double dt, con
     tl_err = "null context";
     return ESC_EINVAL;
   }
-  return engine_adjoint(ctx->e, c0, steps, dt, c_target, lambda_F, ckpt_every, dL_dc0, dL_dparams, L);
+  const double* c0s[1] = {c0};
+  const double* tgs[1] = {c_target};
+  double* outs[1] = {dL_dc0};
+  return engine_adjoint(ctx->e, c0s, steps, dt, tgs, lambda_F, ckpt_every, outs, dL_dparams, L);
+}
+
+esc_status esc_batch_adjoint(esc_batch* b, const double* const* c0, int steps, double dt,
+                             const double* const* c_target, double lambda_F, int ckpt_every, double* const* dL_dc0,
+                             double* dL_dparams, double* L) {
+  if (!b) {
+    tl_err = "null batch";
+    return ESC_EINVAL;
+  }
+  return engine_adjoint(b->e, c0, steps, dt, c_target, lambda_F, ckpt_every, dL_dc0, dL_dparams, L);
 }
 
 int esc_batch_describe(const esc_batch* b, char* buf, int buflen) {

@@ -108,6 +108,9 @@ _SIGNATURES = [
     ("esc_batch_run_device", ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double,
                                             _vp, _i64p]),
     ("esc_batch_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("esc_batch_adjoint", ctypes.c_int, [_vp, ctypes.POINTER(_dp), ctypes.c_int, ctypes.c_double,
+                                         ctypes.POINTER(_dp), ctypes.c_double, ctypes.c_int, ctypes.POINTER(_dp),
+                                         _dp, _dp]),
     ("esc_batch_profile_phases", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                                 _dp]),
@@ -310,6 +313,27 @@ class Batch:
         if st != ESC_OK:
             _raise(st, self._err())
         return [(int(gn[i]), int(gc[i]), [float(x) for x in ms[4 * i:4 * i + 4]]) for i in range(ng.value)]
+
+    def adjoint(self, c0s: Sequence, c_targets: Sequence, dt: float = 0.01, steps: int = 100,
+                lambda_F: float = 1e-3, ckpt_every: int = 0, with_field_gradients: bool = True):
+        """Per particle (L, dL/dc0, dL/d(P, chi, kappa, M0)) for
+        L = 1/2 |c_T - c_target|^2 + lambda_F F[c_T]; all particles must share one grid size.
+        Returns (L array (count,), list of dL/dc0 fields or None, (count, 4) array)."""
+        if len(c0s) != self.count or len(c_targets) != self.count:
+            raise ValueError("one initial field and one target per particle")
+        cs = [_field(c, n, "c0") for c, n in zip(c0s, self.n)]
+        ts = [_field(c, n, "c_target") for c, n in zip(c_targets, self.n)]
+        gs = [np.zeros((n, n)) for n in self.n] if with_field_gradients else None
+        dp = np.zeros((self.count, 4))
+        L = np.zeros(self.count)
+        carr = (_dp * self.count)(*[_ptr(c) for c in cs])
+        tarr = (_dp * self.count)(*[_ptr(c) for c in ts])
+        garr = (_dp * self.count)(*[_ptr(x) for x in gs]) if gs is not None else None
+        st = load_library().esc_batch_adjoint(self._h, carr, int(steps), float(dt), tarr, float(lambda_F),
+                                              int(ckpt_every), garr, _ptr(dp), _ptr(L))
+        if st != ESC_OK:
+            _raise(st, self._err())
+        return L, gs, dp
 
     def describe(self):
         """The autotuner's choice of kernel families per size group (list of dicts)."""

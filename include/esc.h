@@ -123,6 +123,17 @@ esc_status esc_batch_run_device(esc_batch *b, double *const *c, int steps, doubl
 
 esc_status esc_batch_set_stream(esc_batch *b, void *stream);
 
+/* Gradients for a whole batch of one grid size (all n[i] equal; otherwise
+ * ESC_EINVAL): for every particle i the loss, dL/dc0 and dL/d(P, chi, kappa, M0)
+ * of esc_adjoint, computed together (every adjoint kernel runs over all
+ * particles at once).  c0[i], c_target[i] and dL_dc0[i] (n*n each, entries of
+ * dL_dc0 may be NULL) are host arrays; dL_dparams receives count*4 values
+ * (particle-major), L count values; either may be NULL.  No counterpart in the
+ * reference; it serves the batched parameter fit. */
+esc_status esc_batch_adjoint(esc_batch *b, const double *const *c0, int steps, double dt,
+                             const double *const *c_target, double lambda_F, int ckpt_every, double *const *dL_dc0,
+                             double *dL_dparams, double *L);
+
 /* Measurement aid: runs `steps` further steps on the batch's current device state
  * (left by the last run) launching each phase kernel separately between CUDA
  * events, and reports the mean duration in milliseconds of the four phase

@@ -79,3 +79,33 @@ def test_adjoint_mixed_precision_close_to_fp64():
     assert abs(L32 - L64) <= 1e-6 * abs(L64)
     assert np.max(np.abs(g32 - g64)) <= 1e-4 * np.max(np.abs(g64))
     assert np.max(np.abs(th32 - th64) / np.abs(th64)) <= 1e-3
+
+
+def test_batch_adjoint_matches_oracle_per_particle():
+    """esc_batch_adjoint: every particle of a one-size batch gets its own oracle gradient."""
+    n, steps, lamF = 48, 25, 1e-3
+    base = orc.Parameters()
+    ps = [adj._with(base, P=base.P * f, chi=base.chi * g, kappa=base.kappa * k)
+          for f, g, k in [(1.0, 1.0, 1.0), (1.3, 0.8, 1.2), (0.7, 1.2, 0.9)]]
+    c0s, phis, cts = [], [], []
+    for i, p in enumerate(ps):
+        c0, phi = orc.initial_fields(n, radius=n / 4 + i, width=2.0, seed=20 + i)
+        pt = adj._with(p, P=p.P * 1.1, chi=p.chi * 0.9)
+        c0s.append(c0)
+        phis.append(phi)
+        cts.append(adj.forward_states(c0, phi, steps, 0.01, pt)[-1])
+    with esc.Batch(phis, params=[_ep(p) for p in ps], precision="fp64") as b:
+        L, gs, th = b.adjoint(c0s, cts, dt=0.01, steps=steps, lambda_F=lamF, ckpt_every=6)
+    for i, p in enumerate(ps):
+        Lo, go, tho = adj.gradient(c0s[i], phis[i], steps, 0.01, cts[i], lamF, p)
+        assert abs(L[i] - Lo) <= 1e-12 * abs(Lo)
+        assert np.max(np.abs(gs[i] - go)) <= 1e-10 * np.max(np.abs(go))
+        assert np.max(np.abs(th[i] - tho) / np.maximum(np.abs(tho), 1e-30)) <= 1e-9, (i, th[i], tho)
+
+
+def test_batch_adjoint_rejects_mixed_sizes():
+    phis = [orc.particle_disc(32, 1.0, 8.0, 2.0), orc.particle_disc(48, 1.0, 12.0, 2.0)]
+    c0s = [orc.interior_noise(f, 1) for f in phis]
+    with esc.Batch(phis, precision="fp64") as b:
+        with pytest.raises(esc.EscError):
+            b.adjoint(c0s, c0s, steps=3)
