@@ -67,7 +67,6 @@ struct Group {
   void* phi = nullptr;
   void* tw_s = nullptr;
   void* tw_w = nullptr;
-  void* tw_p = nullptr;  // FP32 twiddles duplicated in both lanes (mixed precision)
   double* cio = nullptr;
   double* part = nullptr;
   double* scal = nullptr;
@@ -327,7 +326,6 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
     TRY(E.alloc(&g.phi, cnt * nn * wr, "particle buffer"));
     TRY(E.alloc(&g.tw_s, (size_t)g.n * 2 * sr, "twiddles"));
     TRY(E.alloc(&g.tw_w, (size_t)g.n * 2 * wr, "twiddles"));
-    if (wr == 4) TRY(E.alloc(&g.tw_p, (size_t)g.n * 4 * sizeof(float), "packed twiddles"));
     TRY(E.alloc(&g.cio, cnt * nn * sizeof(double), "field staging"));
     TRY(E.alloc(&g.part, cnt * (size_t)g.ks->part_len * sizeof(double), "partials"));
     TRY(E.alloc(&g.scal, cnt * 4 * sizeof(double), "scalars"));
@@ -346,12 +344,6 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
     } else {
       auto t = twiddles<float>(g.n);
       CK(cudaMemcpy(g.tw_w, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
-      std::vector<float> pk(4 * (size_t)g.n);
-      for (size_t j = 0; j < (size_t)g.n; ++j) {
-        pk[4 * j] = pk[4 * j + 1] = t[2 * j];
-        pk[4 * j + 2] = pk[4 * j + 3] = t[2 * j + 1];
-      }
-      CK(cudaMemcpy(g.tw_p, pk.data(), pk.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     // particle fields in the work precision
     if (wr == 8) {
@@ -386,7 +378,6 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
       d.bad_step = g.bad + s;
       d.tw_s = g.tw_s;
       d.tw_w = g.tw_w;
-      d.tw_p = g.tw_p;
       d.cio = g.cio + s * nn;
     }
     CK(cudaMemset(g.cnt, 0, cnt * 4 * sizeof(unsigned)));

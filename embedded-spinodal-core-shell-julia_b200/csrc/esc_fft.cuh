@@ -101,13 +101,7 @@ __device__ __forceinline__ cpx<double> ldc<double>(const cpx<double>* p) {
 }
 
 // ---- packed pairs of complex values: cpx<f2> holds (x0, x1) + i (y0, y1), two
-// independent transforms in the two lanes.  Twiddle tables for them hold each
-// factor duplicated in both lanes.
-template <>
-__device__ __forceinline__ cpx<f2> ldc<f2>(const cpx<f2>* p) {
-  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-  return mkc<f2>(f2(v.x, v.y), f2(v.z, v.w));
-}
+// independent transforms in the two lanes (twiddles: DupTable below).
 __device__ __forceinline__ cpx<f2> cmul(cpx<f2> a, cpx<f2> b) {
   const f2 nby = b.y * f2(-1.0f, -1.0f);
   return mkc<f2>(fma(a.y, nby, a.x * b.x), fma(a.x, b.y, a.y * b.x));
@@ -347,6 +341,15 @@ struct WarpSync {
 // the non-coherent path).
 template <typename Re>
 __device__ __forceinline__ cpx<Re> tw_at(const cpx<Re>* tw, int i) { return ldc(tw + i); }
+// Packed transforms reading the scalar FP32 table: each factor is loaded once
+// (8 bytes) and placed in both lanes.
+struct DupTable {
+  const cpx<float>* p;
+};
+__device__ __forceinline__ cpx<f2> tw_at(DupTable tw, int i) {
+  const cpx<float> w = ldc(tw.p + i);
+  return mkc<f2>(f2(w.x, w.x), f2(w.y, w.y));
+}
 
 // One Stockham pass (radix RAD, NS = product of earlier radices).
 template <bool INV, class P, int RAD, int NS, bool LAST, class Sync = BlockSync, typename Re, class L, class TW>

@@ -62,7 +62,6 @@ struct InstDev {
   long long* bad_step;
   const void* tw_s;   // twiddles e^{-2 pi i j/n} in SR
   const void* tw_w;   // same in WR
-  const void* tw_p;   // FP32 table with each factor in both lanes of a packed pair (mixed only)
   double* cio;        // real FP64 field for init/final (n*n)
 };
 
@@ -520,7 +519,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
       const cpx<WR> mu = cscale(a[m] + u[m], scale);
       q[m] = pack2(times_i(cscale(mu, kxd)), times_i(cscale(mu, kyd)));
     }
-    fft<true, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, reinterpret_cast<const cpx<f2>*>(I.tw_p));
+    fft<true, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, DupTable{reinterpret_cast<const cpx<float>*>(I.tw_w)});
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       a[m] = lane0(q[m]);
@@ -654,7 +653,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b
     cpx<f2> q[E];
 #pragma unroll
     for (int m = 0; m < E; ++m) q[m] = pack2(a[m], b[m]);
-    fft<false, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, reinterpret_cast<const cpx<f2>*>(I.tw_p));
+    fft<false, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, DupTable{reinterpret_cast<const cpx<float>*>(I.tw_w)});
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       a[m] = lane0(q[m]);

@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w2(const
   }
   cpx<f2>* xs = reinterpret_cast<cpx<f2>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<f2>)> lay{g * N, gw};
-  const cpx<f2>* twp = reinterpret_cast<const cpx<f2>*>(I.tw_p);
+  const DupTable twp{reinterpret_cast<const cpx<float>*>(I.tw_w)};
   fft<true, P, WarpSync>(v, t, xs, lay, twp);
   const f2 Mh(0.5 * I.p.mobility);
   double dsum = 0.0;
