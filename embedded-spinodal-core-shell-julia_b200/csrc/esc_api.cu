@@ -519,6 +519,8 @@ esc_status autotune(Engine& E) {
       else g.row_family = g.warp_rows ? 2 : (g.pipe_rows ? 1 : 0);
       g.col_family = g.pipe_cols ? 1 : 0;
       if (row_family_override() < 0 && pipeline_enabled()) apply_cols(g, 0);
+      const int cfo = col_family_override();
+      if ((cfo == 1 && can_pipe_cols) || (cfo == 2 && g.ks->E_alt != g.ks->E)) apply_cols(g, cfo);
       continue;
     }
     any = true;
