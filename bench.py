@@ -440,7 +440,8 @@ def main():
         v64 = world * pts * args.steps / (ms64 / 1000.0)
         f_final = [w.cpu().numpy() for w in cf]
         max_err = max(float(np.max(np.abs(a - b))) for a, b in zip(bm_final, f_final))
-        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / args.steps, "speedup_mixed_over_fp64": value / v64}
+        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / args.steps, "speedup_mixed_over_fp64": value / v64,
+                "kernel_families": [{k: g[k] for k in ("n", "rows", "cols")} for g in bf.describe()]}
         bf.close()
 
     # ---- end to end through esc_batch_run with pinned host buffers ----

@@ -115,6 +115,10 @@ _SIGNATURES = [
                                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                                 _dp]),
     ("esc_batch_describe", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int]),
+    ("esc_particle_device", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_double,
+                                           _vp, _vp]),
+    ("esc_noise_device", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
+                                        _vp, _vp]),
     ("esc_batch_last_error", ctypes.c_char_p, [_vp]),
     ("esc_batch_destroy", None, [_vp]),
 ]
@@ -144,6 +148,33 @@ def load_library() -> ctypes.CDLL:
             fn.argtypes = args
         _LIB = lib
     return _LIB
+
+
+SHAPES = {"disc": 0, "band": 1, "ellipse": 2, "annulus": 3, "squircle": 4, "elliptic_shell": 5, "elliptic_hole": 6}
+
+
+def particle_device(shape: str, n: int, phi_ptr: int, params, width: float = 2.0, spacing: float = 1.0,
+                    stream_ptr: int = 0) -> None:
+    """Fills the device array at `phi_ptr` (n*n doubles) with a particle shape
+    (esc_particle_device; shapes and parameters as in include/esc.h)."""
+    q = np.zeros(4)
+    q[:len(params)] = params
+    st = load_library().esc_particle_device(SHAPES[shape], int(n), float(spacing), _ptr(q), float(width),
+                                            _vp(phi_ptr), _vp(stream_ptr) if stream_ptr else None)
+    if st != ESC_OK:
+        _raise(st, load_library().esc_last_error(None).decode())
+
+
+def noise_device(n: int, c_ptr: int, seed: int, phi_ptr: int = 0, mean: float = 0.5, amplitude: float = 0.01,
+                 stream_ptr: int = 0) -> None:
+    """Fills the device array at `c_ptr` with counter-based noise (esc_noise_device):
+    inside the particle at `phi_ptr` with its interior mean removed, or over the whole
+    field when phi_ptr is 0."""
+    st = load_library().esc_noise_device(int(n), _vp(phi_ptr) if phi_ptr else None, float(mean), float(amplitude),
+                                         ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), _vp(c_ptr),
+                                         _vp(stream_ptr) if stream_ptr else None)
+    if st != ESC_OK:
+        _raise(st, load_library().esc_last_error(None).decode())
 
 
 def supported_size(n: int) -> bool:

@@ -57,3 +57,54 @@ def initial_fields(n: int, spacing: float = 1.0, radius: float = 70.0, width: fl
     """``initial_fields`` of core_shell.jl:27-37: returns (c, phi)."""
     phi = particle_disc(n, spacing, radius, width)
     return interior_noise(phi, seed), phi
+
+
+# ---- the shape set and the counter-based noise of esc_particle_device / esc_noise_device ----
+
+def _profile(r, R, w):
+    return 0.5 * (1.0 - np.tanh((r - R) / w))
+
+
+def particle(shape: str, n: int, params, width: float = 2.0, spacing: float = 1.0) -> np.ndarray:
+    """Host mirror of esc_particle_device (shapes and parameters as in include/esc.h)."""
+    p = list(params) + [0.0] * (4 - len(params))
+    x = _centred(n, spacing).reshape(1, n)
+    y = _centred(n, spacing).reshape(n, 1)
+    r = np.sqrt(x * x + y * y)
+    w = width
+    if shape == "disc":
+        return _profile(r, p[0], w) + 0.0 * x
+    if shape == "band":
+        return 0.5 * (np.tanh((y - p[0]) / w) - np.tanh((y - p[1]) / w)) + 0.0 * x
+    if shape == "ellipse":
+        return _profile(np.sqrt((x * p[1] / p[0]) ** 2 + y * y), p[1], w)
+    if shape == "annulus":
+        return _profile(r, p[1], w) - _profile(r, p[0], w)
+    if shape == "squircle":
+        return _profile(np.sqrt(np.sqrt(x ** 4 + y ** 4)), p[0], w)
+    if shape == "elliptic_shell":
+        return _profile(np.sqrt((x * p[1] / p[0]) ** 2 + y * y), p[1], w) - _profile(r, p[2], w)
+    if shape == "elliptic_hole":
+        return _profile(r, p[0], w) - _profile(np.sqrt((x * p[2] / p[1]) ** 2 + y * y), p[2], w)
+    raise ValueError(f"unknown shape {shape!r}")
+
+
+def splitmix_uniform(seed: int, count: int) -> np.ndarray:
+    """u_k in [0, 1) for k < count: SplitMix64 of state seed + (k+1) * golden gamma, top 53 bits."""
+    with np.errstate(over="ignore"):
+        k = np.arange(1, count + 1, dtype=np.uint64)
+        z = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + k * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def counter_noise(n: int, seed: int, phi=None, mean: float = 0.5, amplitude: float = 0.01) -> np.ndarray:
+    """Host mirror of esc_noise_device."""
+    e = (amplitude * (2.0 * splitmix_uniform(seed, n * n) - 1.0)).reshape(n, n)
+    if phi is None:
+        return mean + e
+    inside = np.asarray(phi) >= 0.5
+    shift = e[inside].mean() if inside.any() else 0.0
+    return np.where(inside, mean + (e - shift), mean)

@@ -150,6 +150,42 @@ esc_status esc_batch_profile_phases(esc_batch *b, int steps, int *n_groups, int 
 int esc_batch_describe(const esc_batch *b, char *buf, int buflen);
 const char *esc_batch_last_error(const esc_batch *b);
 
+/* Particle shapes for esc_particle_device.  Coordinates x = (i - n/2) dx along
+ * the contiguous index i and y = (j - n/2) dx; S(r, R) = (1 - tanh((r - R)/w))/2.
+ * params holds four values (unused ones ignored):
+ *   DISC           S(r, p0)                                   (core_shell.jl:29-30)
+ *   BAND           (tanh((y - p0)/w) - tanh((y - p1)/w))/2     (band p0 < y < p1)
+ *   ELLIPSE        S(sqrt((x p1/p0)^2 + y^2), p1)             (semi-axes p0 along x, p1 along y)
+ *   ANNULUS        S(r, p1) - S(r, p0)                        (radii p0 < p1)
+ *   SQUIRCLE       S((x^4 + y^4)^(1/4), p0)
+ *   ELLIPTIC_SHELL ellipse (p0, p1) minus a disc of radius p2
+ *   ELLIPTIC_HOLE  disc of radius p0 minus an ellipse (p1 along x, p2 along y)
+ * The last six restate, in physical coordinates, the shape set of the
+ * historical 2-D program of the reference (original/2022-2d/init_conf.cu:77-147). */
+typedef enum {
+  ESC_SHAPE_DISC = 0,
+  ESC_SHAPE_BAND = 1,
+  ESC_SHAPE_ELLIPSE = 2,
+  ESC_SHAPE_ANNULUS = 3,
+  ESC_SHAPE_SQUIRCLE = 4,
+  ESC_SHAPE_ELLIPTIC_SHELL = 5,
+  ESC_SHAPE_ELLIPTIC_HOLE = 6
+} esc_shape;
+
+/* Fills the DEVICE array phi (n*n) with a particle shape of interface width w.
+ * Runs on `stream` (NULL = default) and returns when done.  Replaces the host
+ * generation of core_shell.jl:29-30 for large grids. */
+esc_status esc_particle_device(int shape, int n, double dx, const double *params, double width, double *phi,
+                               void *stream);
+
+/* Fills the DEVICE array c (n*n) with mean + amplitude (2u - 1), u uniform from
+ * SplitMix64(seed, element index).  With a DEVICE particle field phi (n*n), the
+ * noise is applied only where phi >= 0.5 and its mean there is removed, c = mean
+ * elsewhere (core_shell.jl:31-35, with our counter-based generator instead of
+ * MersenneTwister); with phi NULL the whole field is noisy. */
+esc_status esc_noise_device(int n, const double *phi, double mean, double amplitude, uint64_t seed, double *c,
+                            void *stream);
+
 /* Allocation-free single-particle run.  No counterpart in the reference: it
  * exists for callers that may not call cudaMalloc themselves or through this
  * library (device memory owned by another allocator or a fixed budget, or a

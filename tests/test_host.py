@@ -47,3 +47,28 @@ def test_field_shape_checks():
         esc._field(np.zeros((8, 9)), 8, "c0")
     a = esc._field(np.zeros((8, 8), dtype=np.float32), 8, "c0")
     assert a.dtype == np.float64 and a.flags.c_contiguous
+
+
+def test_splitmix_known_answer():
+    """The first SplitMix64 output of state 0 is 0xE220A8397B1DCDAF (published test value)."""
+    from esc import fields
+    u = fields.splitmix_uniform(0, 2)
+    assert u[0] == (0xE220A8397B1DCDAF >> 11) / 9007199254740992.0
+    assert 0.0 <= u[1] < 1.0
+
+
+def test_counter_noise_interior_mean_removed():
+    from esc import fields
+    phi = fields.particle("disc", 64, [20.0])
+    c = fields.counter_noise(64, 7, phi)
+    inside = phi >= 0.5
+    assert abs(c[inside].mean() - 0.5) < 1e-15
+    assert np.all(c[~inside] == 0.5)
+    assert np.max(np.abs(c - 0.5)) <= 0.02
+
+
+def test_host_shapes_match_the_disc_and_ellipse_generators():
+    from esc import fields
+    assert np.array_equal(fields.particle("disc", 32, [10.0], width=4.0), fields.particle_disc(32, 1.0, 10.0, 4.0))
+    assert np.array_equal(fields.particle("ellipse", 48, [20.0, 12.0], width=2.0),
+                          fields.particle_ellipse(48, 20.0, 12.0, 2.0))
