@@ -366,10 +366,25 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
     if (NS > 1) {
       const int k = j % NS;
       constexpr int STEP = N / (NS * RAD);
+      if constexpr (std::is_same<Re, double>::value && RAD >= 8) {
+        // FP64: one table load per butterfly; the other factors are its powers,
+        // built by a product tree of depth <= 4 (a few ulp, far below the tolerances)
+        cpx<Re> w[RAD];
+        w[1] = tw_at(tw, k * STEP);
+        w[2] = cmul(w[1], w[1]);
 #pragma unroll
-      for (int s = 1; s < RAD; ++s) {
-        const cpx<Re> w = tw_at(tw, s * k * STEP);
-        b[s] = INV ? cmulconj(b[s], w) : cmul(b[s], w);
+        for (int s = 3; s < RAD; ++s) {
+          const int hi = 1 << (31 - __builtin_clz(s));  // largest power of two <= s
+          w[s] = (s == hi) ? cmul(w[s / 2], w[s / 2]) : cmul(w[hi], w[s - hi]);
+        }
+#pragma unroll
+        for (int s = 1; s < RAD; ++s) b[s] = INV ? cmulconj(b[s], w[s]) : cmul(b[s], w[s]);
+      } else {
+#pragma unroll
+        for (int s = 1; s < RAD; ++s) {
+          const cpx<Re> w = tw_at(tw, s * k * STEP);
+          b[s] = INV ? cmulconj(b[s], w) : cmul(b[s], w);
+        }
       }
     }
     DFT<RAD, INV, Re>::run(b);
