@@ -73,7 +73,7 @@ __device__ __forceinline__ void adj_accumulate(const AdjDev& A, int counter, int
 
 // ---- column 1 -------------------------------------------------------------------------
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_adj_col1(const AdjDev* __restrict__ adjs) {
+__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col1(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_col1(const AdjDev* __restrict__ 
 
 // ---- column 2 -------------------------------------------------------------------------
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_adj_col2(const AdjDev* __restrict__ adjs) {
+__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col2(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_col2(const AdjDev* __restrict__ 
 
 // ---- row 2 ----------------------------------------------------------------------------
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_adj_row2(const AdjDev* __restrict__ adjs) {
+__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_row2(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, G = RowGeom<P>::G;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_row2(const AdjDev* __restrict__ 
 
 // ---- seed: mu of the final field (column) ---------------------------------------------
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_adj_mu_col(const AdjDev* __restrict__ adjs) {
+__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_mu_col(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   const AdjDev& A = adjs[blockIdx.y];
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_mu_col(const AdjDev* __restrict_
 
 // ---- seed: lam_T = (c_T - c_target) + lamF mu dx^2 (row) --------------------------------
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_adj_seed_row(const AdjDev* __restrict__ adjs) {
+__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_seed_row(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, G = RowGeom<P>::G;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];

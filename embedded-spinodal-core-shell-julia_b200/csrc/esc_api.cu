@@ -866,6 +866,7 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
     if (!A.ks64 || !A.ks64->adj_col1) return E.fail(ESC_EINVAL, "no adjoint kernels for this size");
     CK(A.ks64->prepare());
     CK(A.ks64->prepare_adj());
+    if (A.ks64->warp_rows) CK(A.ks64->prepare_warp());
     A.pstride = (size_t)A.ks64->part_len + 8 * 4096;
     TRY(E.alloc(&A.phi64, cnt * nn * 8, "adjoint phi"));
     TRY(E.alloc(&A.target, cnt * nn * 8, "adjoint target"));
@@ -1066,7 +1067,10 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
     TRY(adjoint_graph(E, 2, b, len, &gx, [&](cudaStream_t cs) {
       for (int j = len - 1; j >= 0; --j) {
         k64->adj_col1(dd + (size_t)j * cnt, cnt, cs);
-        k64->row_b(A.d_bwd, cnt, A.zero, 0, cs);
+        if (k64->warp_rows)
+          k64->row_b_w(A.d_bwd, cnt, A.zero, 0, cs);  // M grad a: the forward row B, warp-independent form
+        else
+          k64->row_b(A.d_bwd, cnt, A.zero, 0, cs);
         k64->adj_col2(dd + (size_t)j * cnt, cnt, cs);
         k64->adj_row2(dd + (size_t)j * cnt, cnt, cs);
       }
