@@ -207,26 +207,35 @@ struct KS {
       k_col_b_p<P, SR, WR><<<grid_for(total, 3), PG::CB, 2 * PG::stage_cb + kStageAlignSlack, st>>>(d, count, *m);
     }
   }
-  // ---- warp-independent rows (their own plan, groups inside one warp) ----
-  using WP = typename WarpPlan<N>::type;
-  static constexpr bool warp_ok = (WP::T <= 32) && (32 % WP::T == 0);
+  // ---- warp-independent rows (their own plans: groups inside one warp, or 64-thread blocks) ----
+  using WPA = typename WarpPlanA<N>::type;  // row A
+  using WP = typename WarpPlan<N>::type;    // row B (and the adjoint's row B)
+  template <class Q>
+  static constexpr bool group_ok() {
+    return ((Q::T <= 32) && (32 % Q::T == 0)) || Q::T == 64;
+  }
+  static constexpr bool warp_ok = group_ok<WPA>() && group_ok<WP>();
+  static size_t warp_smem_a() {
+    if constexpr (warp_ok) return WarpRowGeom<WPA>::template smem<SR>();
+    return 0;
+  }
   static size_t warp_smem() {
     if constexpr (warp_ok) return WarpRowGeom<WP>::template smem<SR>();
     return 0;
   }
-  static int warp_tiles_pairs() {
-    if constexpr (warp_ok) return WarpRowGeom<WP>::tiles_pairs;
-    return 0;
-  }
-  static int warp_tiles_rows() {
-    if constexpr (warp_ok) return WarpRowGeom<WP>::tiles_rows;
+  static int warp_partials() {  // partial slots of the row kernels (row A holds 5 per slot)
+    if constexpr (warp_ok) {
+      const int a = 5 * WarpRowGeom<WPA>::tiles_pairs * WarpRowGeom<WPA>::NW;
+      const int b = WarpRowGeom<WP>::tiles_rows * WarpRowGeom<WP>::NW;
+      return a > b ? a : b;
+    }
     return 0;
   }
   static cudaError_t prepare_warp() {
     if constexpr (warp_ok) {
       cudaError_t e;
-      const int b = (int)warp_smem();
-      if ((e = cudaFuncSetAttribute(k_row_a_w<WP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+      const int a = (int)warp_smem_a(), b = (int)warp_smem();
+      if ((e = cudaFuncSetAttribute(k_row_a_w<WPA, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, a))) return e;
       if ((e = cudaFuncSetAttribute(k_row_b_w<WP, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
       if constexpr (kPackedRows)
         if ((e = cudaFuncSetAttribute(k_row_b_w2<WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
@@ -235,16 +244,17 @@ struct KS {
   }
   static void row_a_w(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
     if constexpr (warp_ok)
-      k_row_a_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kWarpBlock, warp_smem(), st>>>(d, base, s);
+      k_row_a_w<WPA, SR, WR><<<dim3(WarpRowGeom<WPA>::tiles_pairs, count), WarpRowGeom<WPA>::BLOCK, warp_smem_a(),
+                                st>>>(d, base, s);
   }
   // the mixed precision transforms two rows per group in packed FP32 pairs
   static constexpr bool kPackedRows = std::is_same<SR, double>::value && std::is_same<WR, float>::value;
   static void row_b_w(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
     if constexpr (warp_ok) {
       if constexpr (kPackedRows)
-        k_row_b_w2<WP><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), kWarpBlock, warp_smem(), st>>>(d, base, s);
+        k_row_b_w2<WP><<<dim3(WarpRowGeom<WP>::tiles_pairs, count), WarpRowGeom<WP>::BLOCK, warp_smem(), st>>>(d, base, s);
       else
-        k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), kWarpBlock, warp_smem(), st>>>(d, base, s);
+        k_row_b_w<WP, SR, WR><<<dim3(WarpRowGeom<WP>::tiles_rows, count), WarpRowGeom<WP>::BLOCK, warp_smem(), st>>>(d, base, s);
     }
   }
   // ---- alternative column plan ----
@@ -315,9 +325,8 @@ struct KS {
       const int alt_need = 5 * ((H + kBlock / AP::T - 1) / (kBlock / AP::T)) + alt_tiles_cols +
                            (N + kBlock / AP::T - 1) / (kBlock / AP::T);
       if (alt_need > need) need = alt_need;
-      const int wa = 5 * warp_tiles_pairs() * (kWarpBlock / 32), wb = warp_tiles_rows() * (kWarpBlock / 32);
-      if (wa > need) need = wa;
-      if (wb > need) need = wb;
+      const int wab = warp_partials();
+      if (wab > need) need = wab;
       k.part_len = need;
     }
     k.smem = smem();

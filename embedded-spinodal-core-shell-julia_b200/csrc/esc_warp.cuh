@@ -29,6 +29,17 @@ ESC_WPLAN(512, 16, 16, 16, 2)
 ESC_WPLAN(768, 24, 8, 8, 12)
 #undef ESC_WPLAN
 
+// Row A (FP64 inverse transform, bulk terms, FP32 forward transform) prefers
+// E8 in 64-thread groups at n = 512: half the registers, 24 warps per SM.
+template <int N>
+struct WarpPlanA {
+  using type = typename WarpPlan<N>::type;
+};
+template <>
+struct WarpPlanA<512> {
+  using type = Plan<512, 8, Radices<8, 8, 8>>;
+};
+
 // Blocks of the warp-independent kernels: no block-wide barrier ties their
 // warps together, so small blocks let every warp start as soon as one retires
 // and keep the warps of an SM spread over load and compute phases.
@@ -38,18 +49,33 @@ ESC_WPLAN(768, 24, 8, 8, 12)
 constexpr int kWarpBlock = ESC_WARP_BLOCK;
 constexpr int kWarpBlocksPerSM = 512 / kWarpBlock;  // 16 warps per SM at up to 128 registers
 
+// Groups of T <= 32 threads live inside one warp (one-warp blocks, __syncwarp).
+// Groups of 64 threads are a whole two-warp block (__syncthreads): E8 plans of
+// the larger sizes, with half the registers per thread of the E16 plans.
 template <class P>
 struct WarpRowGeom {
   static constexpr int N = P::N, T = P::T, H = N / 2;
-  static_assert(T <= 32 && 32 % T == 0, "warp kernels need groups inside one warp");
-  static constexpr int GPW = 32 / T;            // groups per warp
-  static constexpr int NW = kWarpBlock / 32;    // warps per block
-  static constexpr int G = GPW * NW;            // groups per block
+  static constexpr bool kInWarp = T <= 32;
+  static_assert((kInWarp && 32 % T == 0) || T == 64, "groups inside one warp, or a 64-thread block");
+  static constexpr int BLOCK = kInWarp ? kWarpBlock : T;  // threads per block
+  static constexpr int MINB = kInWarp ? kWarpBlocksPerSM : (P::E <= 8 ? 12 : 8);  // blocks per SM compiled for
+  static constexpr int GPW = kInWarp ? 32 / T : 1;        // groups per warp
+  static constexpr int NW = BLOCK / 32;                   // warps per block
+  static constexpr int G = kInWarp ? GPW * NW : 1;        // groups per block
   static constexpr int tiles_pairs = (H + G - 1) / G;
   static constexpr int tiles_rows = (N + G - 1) / G;
+  using Sync = typename std::conditional<kInWarp, WarpSync, BlockSync>::type;
+  static __device__ __forceinline__ void group_sync() { Sync::sync(); }
+  // this thread's index inside its group, and the group's index inside the warp and the block
+  static __device__ __forceinline__ int thread_in_group() { return kInWarp ? (threadIdx.x & 31) % T : threadIdx.x; }
+  static __device__ __forceinline__ int group_in_warp() { return kInWarp ? (threadIdx.x & 31) / T : 0; }
+  static __device__ __forceinline__ int group_in_block() {
+    return kInWarp ? (threadIdx.x >> 5) * GPW + group_in_warp() : 0;
+  }
   template <typename SR>
   static constexpr size_t smem() {
-    return (size_t)G * N * sizeof(cpx<SR>);
+    // the group's exchange slice; a 64-thread group also splits its output through it
+    return (size_t)G * (kInWarp ? N : N + N / 16 + 1) * sizeof(cpx<SR>);
   }
 };
 
@@ -100,7 +126,7 @@ __device__ __forceinline__ bool warp_instance_running(const int* status) {
 
 // =====================================================================================
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_a_w(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k_row_a_w(const InstDev* __restrict__ insts,
                                                        const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
@@ -109,8 +135,8 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_a_w(const 
   const InstDev& I = insts[blockIdx.y];
   if (!warp_instance_running(I.status)) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int t = lane % T, gw = lane / T;           // group inside the warp
-  const int g = warp * GPW + gw;                   // group inside the block
+  const int t = WG::thread_in_group(), gw = WG::group_in_warp();  // thread and group inside the warp
+  const int g = WG::group_in_block();                               // group inside the block
   const int pair = blockIdx.x * G + g;
   const bool active = pair < H;
   const int ya = 2 * pair;
@@ -131,7 +157,7 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_a_w(const 
   }
   cpx<SR>* xs = reinterpret_cast<cpx<SR>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<SR>)> lay_s{g * N, gw};
-  fft<true, P, WarpSync>(v, t, xs, lay_s, reinterpret_cast<const cpx<SR>*>(I.tw_s));
+  fft<true, P, typename WG::Sync>(v, t, xs, lay_s, reinterpret_cast<const cpx<SR>*>(I.tw_s));
 
   const ModelParams mp = I.p;
   const SR invN = (SR)1 / (SR)N;
@@ -182,10 +208,10 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_a_w(const 
   cpx<WR>* xw = reinterpret_cast<cpx<WR>*>(smraw);
   // the FP32 exchange reuses the group's slice (n elements of the smaller type)
   const SwizzleLayout<N, sizeof(cpx<WR>)> lay_w{g * N * (int)(sizeof(cpx<SR>) / sizeof(cpx<WR>)), gw};
-  __syncwarp();
-  fft<false, P, WarpSync>(wv, t, xw, lay_w, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  WG::group_sync();
+  fft<false, P, typename WG::Sync>(wv, t, xw, lay_w, reinterpret_cast<const cpx<WR>*>(I.tw_w));
   cpx<WR> xa[E / 2], xb[E / 2];
-  split_rows<P, WR>(wv, t, nullptr, RowLayout<N>{0}, xa, xb);
+  split_rows<P, WR>(wv, t, xw, RowLayout<N>{0}, xa, xb);
   if (active) {
     cpx<WR>* F = reinterpret_cast<cpx<WR>*>(I.F) + (size_t)ya * H;
 #pragma unroll
@@ -235,7 +261,7 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_a_w(const 
 
 // =====================================================================================
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k_row_b_w(const InstDev* __restrict__ insts,
                                                        const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
@@ -244,8 +270,8 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w(const 
   const InstDev& I = insts[blockIdx.y];
   if (!warp_instance_running(I.status)) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int t = lane % T, gw = lane / T;
-  const int g = warp * GPW + gw;
+  const int t = WG::thread_in_group(), gw = WG::group_in_warp();
+  const int g = WG::group_in_block();
   const int y = blockIdx.x * G + g;
   const bool active = y < N;
   cpx2<WR>* row = reinterpret_cast<cpx2<WR>*>(I.G) + (size_t)(active ? y : 0) * H;
@@ -263,7 +289,7 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w(const 
   }
   cpx<WR>* xw = reinterpret_cast<cpx<WR>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<WR>)> lay{g * N, gw};
-  fft<true, P, WarpSync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  fft<true, P, typename WG::Sync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
   const WR* phi = reinterpret_cast<const WR*>(I.phi);
   const WR M0 = (WR)I.p.mobility;
   double dsum = 0.0;
@@ -276,10 +302,10 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w(const 
     }
     v[m] = cscale(v[m], M);
   }
-  fft<false, P, WarpSync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  fft<false, P, typename WG::Sync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
   cpx<WR> xa[E / 2], xb[E / 2];
-  split_rows<P, WR>(v, t, nullptr, RowLayout<N>{0}, xa, xb);
-  __syncwarp();  // every lane of the group has read its inputs before the row is overwritten
+  split_rows<P, WR>(v, t, xw, RowLayout<N>{0}, xa, xb);
+  WG::group_sync();  // every thread of the group has read its inputs before the row is overwritten
   if (active) {
 #pragma unroll
     for (int m = 0; m < E / 2; ++m) {
@@ -342,8 +368,34 @@ __device__ __forceinline__ void split_rows_packed(const cpx<f2> (&y)[P::E], int 
   }
 }
 
+// the same split for a block-sized group: the mirror modes go through the group's slice
 template <class P>
-__global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w2(const InstDev* __restrict__ insts,
+__device__ __forceinline__ void split_rows_packed_block(const cpx<f2> (&y)[P::E], int t, cpx<f2>* slice,
+                                                        cpx<f2> (&xa)[P::E / 2], cpx<f2> (&xb)[P::E / 2]) {
+  constexpr int N = P::N, E = P::E, T = P::T;
+#pragma unroll
+  for (int m = E / 2; m < E; ++m) slice[t + T * m] = y[m];
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < E / 2; ++m) {
+    const cpx<f2> y1 = y[m];
+    cpx<f2> y2 = slice[(N - t - T * m) % N];
+    if (t == 0) {
+      if (m == 0) {
+        const cpx<f2> yh = y[E / 2];
+        xa[0] = mkc<f2>(y1.x + y1.x, yh.x + yh.x);
+        xb[0] = mkc<f2>(y1.y + y1.y, yh.y + yh.y);
+        continue;
+      }
+      y2 = y[E - m];
+    }
+    xa[m] = mkc<f2>(y1.x + y2.x, y1.y - y2.y);
+    xb[m] = mkc<f2>(y1.y + y2.y, y2.x - y1.x);
+  }
+}
+
+template <class P>
+__global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k_row_b_w2(const InstDev* __restrict__ insts,
                                                         const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
@@ -352,8 +404,8 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w2(const
   const InstDev& I = insts[blockIdx.y];
   if (!warp_instance_running(I.status)) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int t = lane % T, gw = lane / T;
-  const int g = warp * GPW + gw;
+  const int t = WG::thread_in_group(), gw = WG::group_in_warp();
+  const int g = WG::group_in_block();
   const int pair = blockIdx.x * G + g;
   const bool active = pair < H;
   const int y0 = 2 * (active ? pair : 0);
@@ -375,7 +427,7 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w2(const
   cpx<f2>* xs = reinterpret_cast<cpx<f2>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<f2>)> lay{g * N, gw};
   const DupTable twp{reinterpret_cast<const cpx<float>*>(I.tw_w)};
-  fft<true, P, WarpSync>(v, t, xs, lay, twp);
+  fft<true, P, typename WG::Sync>(v, t, xs, lay, twp);
   const f2 Mh(0.5 * I.p.mobility);
   double dsum = 0.0;
 #pragma unroll
@@ -391,10 +443,13 @@ __global__ void __launch_bounds__(kWarpBlock, kWarpBlocksPerSM) k_row_b_w2(const
     }
     v[m] = mkc<f2>(v[m].x * M, v[m].y * M);
   }
-  __syncwarp();  // every lane of the group has finished its gathers before the next scatter
-  fft<false, P, WarpSync>(v, t, xs, lay, twp);
+  WG::group_sync();  // every thread of the group has finished its gathers before the next scatter
+  fft<false, P, typename WG::Sync>(v, t, xs, lay, twp);
   cpx<f2> xa[E / 2], xb[E / 2];
-  split_rows_packed<P>(v, t, xa, xb);
+  if constexpr (WG::kInWarp)
+    split_rows_packed<P>(v, t, xa, xb);
+  else
+    split_rows_packed_block<P>(v, t, xs, xa, xb);
   if (active) {
 #pragma unroll
     for (int m = 0; m < E / 2; ++m) {
