@@ -129,7 +129,7 @@ template <class P, typename SR, typename WR>
 __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k_row_a_w(const InstDev* __restrict__ insts,
                                                        const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
-  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, NW = WG::NW, G = WG::G;
   constexpr int tiles = WG::tiles_pairs;
   extern __shared__ __align__(16) unsigned char smraw[];
   const InstDev& I = insts[blockIdx.y];
@@ -264,7 +264,7 @@ template <class P, typename SR, typename WR>
 __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k_row_b_w(const InstDev* __restrict__ insts,
                                                        const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
-  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, NW = WG::NW, G = WG::G;
   constexpr int tiles = WG::tiles_rows;
   extern __shared__ __align__(16) unsigned char smraw[];
   const InstDev& I = insts[blockIdx.y];
@@ -398,7 +398,7 @@ template <class P>
 __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k_row_b_w2(const InstDev* __restrict__ insts,
                                                         const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
-  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, GPW = WG::GPW, NW = WG::NW, G = WG::G;
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, NW = WG::NW, G = WG::G;
   constexpr int tiles = WG::tiles_pairs;
   extern __shared__ __align__(16) unsigned char smraw[];
   const InstDev& I = insts[blockIdx.y];
