@@ -345,6 +345,8 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
       auto t = twiddles<float>(g.n);
       CK(cudaMemcpy(g.tw_w, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
+    g.ks->fill_tables(g.tw_s, g.tw_w, E.own);
+    CK(cudaGetLastError());
     // particle fields in the work precision
     if (wr == 8) {
       for (size_t s = 0; s < cnt; ++s)
@@ -899,6 +901,9 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
       CK(cudaMemcpy(A.phi64, pd.data(), cnt * nn * 8, cudaMemcpyHostToDevice));
     }
     if (g.ks->sr_bytes == 8) CK(cudaMemcpy(A.tw64, g.tw_s, (size_t)n * 16, cudaMemcpyDeviceToDevice));
+    A.ks64->fill_tables(A.tw64, A.tw64, st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
     CK(cudaMemset(A.zero, 0, 4));
     A.ready = true;
   }

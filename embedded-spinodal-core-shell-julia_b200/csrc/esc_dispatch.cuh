@@ -17,6 +17,9 @@ struct KernelSet {
   size_t sr_bytes, wr_bytes;  // sizeof(real) of the state and work types
   cudaError_t (*prepare)();
   cudaError_t (*prepare_pipe)();
+  // fills the pass-major twiddle tables of every plan the set uses from the
+  // plain tables (state and work precision), in stream order
+  void (*fill_tables)(const void*, const void*, cudaStream_t);
   void (*init)(const InstDev*, int, cudaStream_t);
   void (*fin)(const InstDev*, int, cudaStream_t);
   void (*row_a)(const InstDev*, int, const int*, int, cudaStream_t);
@@ -279,6 +282,22 @@ struct KS {
   static void col_b_alt(const InstDev* d, int count, cudaStream_t st) {
     k_col_b<AP, SR, WR><<<dim3(alt_tiles_cols, count), kBlock, alt_smem(), st>>>(d);
   }
+  // ---- pass-major twiddle tables ----
+  template <class Q, typename Re>
+  static void fill_one(const void* tw, cudaStream_t st) {
+    k_fill_pass_tw<Q, Re><<<1, 256, 0, st>>>(static_cast<const cpx<Re>*>(tw));
+  }
+  static void fill_tables(const void* tw_s, const void* tw_w, cudaStream_t st) {
+    fill_one<P, SR>(tw_s, st);
+    fill_one<P, WR>(tw_w, st);
+    fill_one<AP, SR>(tw_s, st);
+    fill_one<AP, WR>(tw_w, st);
+    if constexpr (warp_ok) {
+      fill_one<WPA, SR>(tw_s, st);
+      fill_one<WPA, WR>(tw_w, st);
+      fill_one<WP, WR>(tw_w, st);
+    }
+  }
   // ---- adjoint (FP64) ----
   static constexpr bool adj_ok = std::is_same<SR, double>::value && std::is_same<WR, double>::value;
   static cudaError_t prepare_adj() {
@@ -333,6 +352,7 @@ struct KS {
     k.sr_bytes = sizeof(SR);
     k.wr_bytes = sizeof(WR);
     k.prepare = &prepare;
+    k.fill_tables = &fill_tables;
     k.init = &init;
     k.fin = &fin;
     k.row_a = &row_a;

@@ -351,8 +351,73 @@ __device__ __forceinline__ cpx<f2> tw_at(DupTable tw, int i) {
   return mkc<f2>(f2(w.x, w.x), f2(w.y, w.y));
 }
 
-// One Stockham pass (radix RAD, NS = product of earlier radices).
-template <bool INV, class P, int RAD, int NS, bool LAST, class Sync = BlockSync, typename Re, class L, class TW>
+// Pass-major twiddle tables, one per plan and precision.  The pass with
+// radix RAD after earlier radices of product NS needs, for butterfly k < NS,
+// the factors w^{s k STEP} (STEP = N / (NS RAD), 0 < s < RAD).  In the plain
+// table e^{-2 pi i j / N} the lanes of a warp (consecutive k) read entries
+// s STEP apart, one sector each once s STEP reaches 4; here factor s of
+// butterfly k sits at OFF + (s - 1) NS + k, so the lanes read consecutive
+// entries.  OFF is the sum of (R - 1) NS' over the earlier passes, and the
+// passes fill exactly N - 1 entries.  The values are copied from the plain
+// table (`k_fill_pass_tw`), so both give the same bits.
+template <class P, typename Re>
+__device__ cpx<Re> g_pass_tw[P::N];
+
+template <class P, typename Re>
+struct PassTable {};  // scalar transforms of plan P read g_pass_tw<P, Re>
+template <class P>
+struct PassTableDup {};  // packed FP32 transforms of plan P: g_pass_tw<P, float>, broadcast into both lanes
+
+// factor s of butterfly k in the pass (NS, RAD) whose pass-major offset is OFF
+template <int N, int NS, int RAD, int OFF, typename Re>
+__device__ __forceinline__ cpx<Re> pass_tw(const cpx<Re>* tw, int k, int s) {
+  return tw_at(tw, s * k * (N / (NS * RAD)));
+}
+template <int N, int NS, int RAD, int OFF>
+__device__ __forceinline__ cpx<f2> pass_tw(DupTable tw, int k, int s) {
+  return tw_at(tw, s * k * (N / (NS * RAD)));
+}
+template <int N, int NS, int RAD, int OFF, class P, typename Re>
+__device__ __forceinline__ cpx<Re> pass_tw(PassTable<P, Re>, int k, int s) {
+  return ldc(&g_pass_tw<P, Re>[OFF + (s - 1) * NS + k]);
+}
+template <int N, int NS, int RAD, int OFF, class P>
+__device__ __forceinline__ cpx<f2> pass_tw(PassTableDup<P>, int k, int s) {
+  const cpx<float> w = ldc(&g_pass_tw<P, float>[OFF + (s - 1) * NS + k]);
+  return mkc<f2>(f2(w.x, w.x), f2(w.y, w.y));
+}
+
+// Copies the plain table tw (e^{-2 pi i j / N}, j < N) into g_pass_tw<P, Re>; one block.
+template <class P, typename Re, int... Rs>
+__device__ __forceinline__ void fill_pass_tw(const cpx<Re>* tw, Radices<Rs...>) {
+  constexpr int rs[] = {Rs...};
+  int ns = 1, off = 0;
+#pragma unroll
+  for (int q = 0; q < (int)sizeof...(Rs); ++q) {
+    const int r = rs[q], step = P::N / (ns * r);
+    for (int e = threadIdx.x; e < (r - 1) * ns; e += blockDim.x) {
+      const int s = 1 + e / ns, k = e % ns;
+      g_pass_tw<P, Re>[off + e] = tw[s * k * step];
+    }
+    off += (r - 1) * ns;
+    ns *= r;
+  }
+}
+template <class P, typename Re>
+__global__ void k_fill_pass_tw(const cpx<Re>* tw) {
+  fill_pass_tw<P, Re>(tw, typename P::List{});
+}
+
+#ifndef ESC_FP64_TREE
+#define ESC_FP64_TREE 1
+#endif
+// FP64 passes of radix >= 8 load one factor per butterfly and build the others as its powers
+constexpr bool kFP64PowerTree = ESC_FP64_TREE != 0;
+
+// One Stockham pass (radix RAD, NS = product of earlier radices, OFF = its
+// offset in a pass-major table).
+template <bool INV, class P, int RAD, int NS, int OFF, bool LAST, class Sync = BlockSync, typename Re, class L,
+          class TW>
 __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay, const TW& tw) {
   constexpr int N = P::N, E = P::E, T = P::T;
   constexpr int NB = E / RAD;
@@ -365,12 +430,11 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
     for (int s = 0; s < RAD; ++s) b[s] = v[q + s * NB];
     if (NS > 1) {
       const int k = j % NS;
-      constexpr int STEP = N / (NS * RAD);
-      if constexpr (std::is_same<Re, double>::value && RAD >= 8) {
+      if constexpr (kFP64PowerTree && std::is_same<Re, double>::value && RAD >= 8) {
         // FP64: one table load per butterfly; the other factors are its powers,
         // built by a product tree of depth <= 4 (a few ulp, far below the tolerances)
         cpx<Re> w[RAD];
-        w[1] = tw_at(tw, k * STEP);
+        w[1] = pass_tw<N, NS, RAD, OFF>(tw, k, 1);
         w[2] = cmul(w[1], w[1]);
 #pragma unroll
         for (int s = 3; s < RAD; ++s) {
@@ -382,7 +446,7 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
       } else {
 #pragma unroll
         for (int s = 1; s < RAD; ++s) {
-          const cpx<Re> w = tw_at(tw, s * k * STEP);
+          const cpx<Re> w = pass_tw<N, NS, RAD, OFF>(tw, k, s);
           b[s] = INV ? cmulconj(b[s], w) : cmul(b[s], w);
         }
       }
@@ -405,20 +469,22 @@ __device__ __forceinline__ void stockham_pass(cpx<Re> (&v)[P::E], int t, cpx<Re>
   }
 }
 
-template <bool INV, class P, int NS, class Sync, typename Re, class L, class TW, int RAD, int... REST>
+template <bool INV, class P, int NS, int OFF, class Sync, typename Re, class L, class TW, int RAD, int... REST>
 __device__ __forceinline__ void fft_passes(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay, const TW& tw,
                                            Radices<RAD, REST...>) {
   constexpr bool LAST = sizeof...(REST) == 0;
-  stockham_pass<INV, P, RAD, NS, LAST, Sync>(v, t, sm, lay, tw);
-  if constexpr (!LAST) fft_passes<INV, P, NS * RAD, Sync>(v, t, sm, lay, tw, Radices<REST...>{});
+  stockham_pass<INV, P, RAD, NS, OFF, LAST, Sync>(v, t, sm, lay, tw);
+  if constexpr (!LAST) fft_passes<INV, P, NS * RAD, OFF + (RAD - 1) * NS, Sync>(v, t, sm, lay, tw, Radices<REST...>{});
 }
 
 // Length-N DFT of the values v[m] at positions t + T*m; result in the same slots.
-// tw: table of e^{-2 pi i j / N}, j < N, in global memory (read through L1).
+// tw: table of e^{-2 pi i j / N}, j < N, in global memory (read through L1), the
+// same broadcast into both lanes (DupTable), or the plan's pass-major table
+// (PassTable, PassTableDup).
 // Every thread of the CTA must call this (it contains __syncthreads).
 template <bool INV, class P, class Sync = BlockSync, typename Re, class L, class TW>
 __device__ __forceinline__ void fft(cpx<Re> (&v)[P::E], int t, cpx<Re>* sm, const L& lay, const TW& tw) {
-  fft_passes<INV, P, 1, Sync>(v, t, sm, lay, tw, typename P::List{});
+  fft_passes<INV, P, 1, 0, Sync>(v, t, sm, lay, tw, typename P::List{});
 }
 
 // Exchange layout of one warp-local FFT group: n elements at `base`, XOR

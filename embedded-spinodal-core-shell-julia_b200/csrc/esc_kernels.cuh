@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
     for (int m = 0; m < E; ++m) v[m] = active ? ldc(S + (size_t)(t + T * m) * H + kx) : mkc<SR>(0, 0);
   }
   cpx<SR>* sms = reinterpret_cast<cpx<SR>*>(smraw);
-  fft<false, P>(v, t, sms, lay, reinterpret_cast<const cpx<SR>*>(I.tw_s));
+  fft<false, P>(v, t, sms, lay, PassTable<P, SR>{});
 
   const bool packed_tile = blockIdx.x == 0;  // holds kx = 0 (DC + i Nyquist)
   const bool packed = packed_tile && w == 0;
@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
     for (int m = 0; m < E; ++m) a[m] = active ? ldc(F + (size_t)(t + T * m) * H + kx) : mkc<WR>(0, 0);
   }
   cpx<WR>* smw = reinterpret_cast<cpx<WR>*>(smraw);
-  fft<false, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  fft<false, P>(a, t, smw, lay, PassTable<P, WR>{});
   const WR scale = (WR)(1.0 / ((double)N * (double)N));
   const WR kxd = (WR)kxf;  // kx < n/2: never the Nyquist
   if constexpr (kSplitMixed<SR, WR>) {
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
       const cpx<WR> mu = cscale(a[m] + u[m], scale);
       q[m] = pack2(times_i(cscale(mu, kxd)), times_i(cscale(mu, kyd)));
     }
-    fft<true, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, DupTable{reinterpret_cast<const cpx<float>*>(I.tw_w)});
+    fft<true, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, PassTableDup<P>{});
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       a[m] = lane0(q[m]);
@@ -534,8 +534,8 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
       a[m] = times_i(cscale(mu, kxd));   // x-derivative
       u[m] = times_i(cscale(mu, kyd));   // y-derivative
     }
-    fft<true, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
-    fft<true, P>(u, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+    fft<true, P>(a, t, smw, lay, PassTable<P, WR>{});
+    fft<true, P>(u, t, smw, lay, PassTable<P, WR>{});
   }
   if (active) {
     cpx2<WR>* Gp = reinterpret_cast<cpx2<WR>*>(I.G);
@@ -653,15 +653,15 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b
     cpx<f2> q[E];
 #pragma unroll
     for (int m = 0; m < E; ++m) q[m] = pack2(a[m], b[m]);
-    fft<false, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, DupTable{reinterpret_cast<const cpx<float>*>(I.tw_w)});
+    fft<false, P>(q, t, reinterpret_cast<cpx<f2>*>(smraw), lay, PassTableDup<P>{});
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       a[m] = lane0(q[m]);
       b[m] = lane1(q[m]);
     }
   } else {
-    fft<false, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
-    fft<false, P>(b, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+    fft<false, P>(a, t, smw, lay, PassTable<P, WR>{});
+    fft<false, P>(b, t, smw, lay, PassTable<P, WR>{});
   }
   const double c1 = 2.0 * I.p.Q * I.p.kappa * I.dt;  // den = 1 + c1 k2^2
   const double kxf = kunit * (double)kx;
@@ -711,7 +711,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b
       a[m] = cscale(div, iden * dtn);
     }
   }
-  fft<true, P>(a, t, smw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  fft<true, P>(a, t, smw, lay, PassTable<P, WR>{});
   // exact mass conservation: the DC row-mode increments (packed column, real
   // part) must sum to zero over y; remove the rounding residue in FP64.
   double corr = 0.0;

@@ -163,6 +163,7 @@ extern "C" esc_status esc_run_noalloc(int n, double dx, const double* phi, const
     if (e_ != cudaSuccess) return fail(ESC_ECUDA, #call, e_); \
   } while (0)
   NA_CK(cudaMemcpyAsync(base + kOffTw, tw, (size_t)n * 16, cudaMemcpyHostToDevice, st));
+  ks->fill_tables(base + kOffTw, base + kOffTw, st);  // the pass-major tables are fixed __device__ arrays too
   NA_CK(cudaMemcpyAsync(base + kOffInst, &d, sizeof d, cudaMemcpyHostToDevice, st));
   // state that must start at zero: counters, status, bad step (-1), step counter
   NA_CK(cudaMemsetAsync(base + kOffCnt, 0, 256, st));

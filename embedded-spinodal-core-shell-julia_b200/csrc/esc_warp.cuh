@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   }
   cpx<SR>* xs = reinterpret_cast<cpx<SR>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<SR>)> lay_s{g * N, gw};
-  fft<true, P, typename WG::Sync>(v, t, xs, lay_s, reinterpret_cast<const cpx<SR>*>(I.tw_s));
+  fft<true, P, typename WG::Sync>(v, t, xs, lay_s, PassTable<P, SR>{});
 
   const ModelParams mp = I.p;
   const SR invN = (SR)1 / (SR)N;
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   // the FP32 exchange reuses the group's slice (n elements of the smaller type)
   const SwizzleLayout<N, sizeof(cpx<WR>)> lay_w{g * N * (int)(sizeof(cpx<SR>) / sizeof(cpx<WR>)), gw};
   WG::group_sync();
-  fft<false, P, typename WG::Sync>(wv, t, xw, lay_w, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  fft<false, P, typename WG::Sync>(wv, t, xw, lay_w, PassTable<P, WR>{});
   cpx<WR> xa[E / 2], xb[E / 2];
   split_rows<P, WR>(wv, t, xw, RowLayout<N>{0}, xa, xb);
   if (active) {
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   }
   cpx<WR>* xw = reinterpret_cast<cpx<WR>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<WR>)> lay{g * N, gw};
-  fft<true, P, typename WG::Sync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  fft<true, P, typename WG::Sync>(v, t, xw, lay, PassTable<P, WR>{});
   const WR* phi = reinterpret_cast<const WR*>(I.phi);
   const WR M0 = (WR)I.p.mobility;
   double dsum = 0.0;
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
     }
     v[m] = cscale(v[m], M);
   }
-  fft<false, P, typename WG::Sync>(v, t, xw, lay, reinterpret_cast<const cpx<WR>*>(I.tw_w));
+  fft<false, P, typename WG::Sync>(v, t, xw, lay, PassTable<P, WR>{});
   cpx<WR> xa[E / 2], xb[E / 2];
   split_rows<P, WR>(v, t, xw, RowLayout<N>{0}, xa, xb);
   WG::group_sync();  // every thread of the group has read its inputs before the row is overwritten
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   }
   cpx<f2>* xs = reinterpret_cast<cpx<f2>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<f2>)> lay{g * N, gw};
-  const DupTable twp{reinterpret_cast<const cpx<float>*>(I.tw_w)};
+  const PassTableDup<P> twp{};
   fft<true, P, typename WG::Sync>(v, t, xs, lay, twp);
   const f2 Mh(0.5 * I.p.mobility);
   double dsum = 0.0;
