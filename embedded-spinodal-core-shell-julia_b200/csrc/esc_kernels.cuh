@@ -260,10 +260,11 @@ struct ColGeom {
 };
 // Resident blocks per SM the column kernels are compiled for: the mixed
 // precision's transforms fit 3 blocks at up to 8 elements per thread and 2 at
-// up to 16; larger plans (and the FP64 drop-in) keep the compiler's choice.
+// up to 16; the FP64 drop-in fits 2 at up to 8; larger plans keep the
+// compiler's choice.
 template <class P, typename SR, typename WR>
 constexpr int col_min_blocks() {
-  return kSplitMixed<SR, WR> ? (P::E <= 8 ? 3 : (P::E <= 16 ? 2 : 1)) : 1;
+  return kSplitMixed<SR, WR> ? (P::E <= 8 ? 3 : (P::E <= 16 ? 2 : 1)) : (P::E <= 8 ? 2 : 1);
 }
 
 // init: c (FP64 real) -> S (packed x-transform), one row pair per group
