@@ -108,14 +108,50 @@ __device__ __forceinline__ bool warp_arrive_last(unsigned* counter, unsigned tot
   return last != 0;
 }
 
-// deterministic warp fold of `count` partials spaced `stride` apart
+// deterministic warp fold of `count` partials spaced `stride` apart.  The fold
+// runs in the last warp of an instance, and the last instance's fold ends the
+// launch, so its loads are unrolled to keep several in flight; each lane still
+// accumulates in increasing slot order.
 template <class Op>
 __device__ __forceinline__ double warp_fold(const double* p, int count, int stride, double init) {
   double v = init;
+#pragma unroll 8
   for (int i = (threadIdx.x & 31); i < count; i += 32) v = Op::ap(v, __ldcg(p + (size_t)i * stride));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = Op::ap(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+
+// The five row-A folds (sum c, min c, max c, sum f, non-finite count) of slots
+// holding five consecutive doubles, in one pass: one slot's five loads are
+// issued together, with the per-lane order and the shuffle trees of five
+// separate warp_fold calls, so the results are the same bits.
+__device__ __forceinline__ void warp_fold_row_a(const double* p, int count, double& a_sum, double& a_min,
+                                                double& a_max, double& a_f, double& a_bad) {
+  double s0 = 0.0, s1 = INFINITY, s2 = -INFINITY, s3 = 0.0, s4 = 0.0;
+#pragma unroll 4
+  for (int i = (threadIdx.x & 31); i < count; i += 32) {
+    const double* q = p + (size_t)i * 5;
+    const double v0 = __ldcg(q), v1 = __ldcg(q + 1), v2 = __ldcg(q + 2), v3 = __ldcg(q + 3), v4 = __ldcg(q + 4);
+    s0 = OpSum::ap(s0, v0);
+    s1 = OpMin::ap(s1, v1);
+    s2 = OpMax::ap(s2, v2);
+    s3 = OpSum::ap(s3, v3);
+    s4 = OpSum::ap(s4, v4);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 = OpSum::ap(s0, __shfl_xor_sync(0xffffffffu, s0, o));
+    s1 = OpMin::ap(s1, __shfl_xor_sync(0xffffffffu, s1, o));
+    s2 = OpMax::ap(s2, __shfl_xor_sync(0xffffffffu, s2, o));
+    s3 = OpSum::ap(s3, __shfl_xor_sync(0xffffffffu, s3, o));
+    s4 = OpSum::ap(s4, __shfl_xor_sync(0xffffffffu, s4, o));
+  }
+  a_sum = s0;
+  a_min = s1;
+  a_max = s2;
+  a_f = s3;
+  a_bad = s4;
 }
 
 __device__ __forceinline__ bool warp_instance_running(const int* status) {
@@ -236,11 +272,8 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   }
   if (!warp_arrive_last(&I.cnt[0], (unsigned)(tiles * NW))) return;
   const int nslots = tiles * NW;
-  const double a_sum = warp_fold<OpSum>(I.part + 0, nslots, 5, 0.0);
-  const double a_min = warp_fold<OpMin>(I.part + 1, nslots, 5, INFINITY);
-  const double a_max = warp_fold<OpMax>(I.part + 2, nslots, 5, -INFINITY);
-  const double a_f = warp_fold<OpSum>(I.part + 3, nslots, 5, 0.0);
-  const double a_bad = warp_fold<OpSum>(I.part + 4, nslots, 5, 0.0);
+  double a_sum, a_min, a_max, a_f, a_bad;
+  warp_fold_row_a(I.part, nslots, a_sum, a_min, a_max, a_f, a_bad);
   if (lane == 0) {
     const int s = step_index(base, s_local);
     if (I.hist) {
