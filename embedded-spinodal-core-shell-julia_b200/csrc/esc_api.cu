@@ -679,6 +679,9 @@ esc_status ensure_graph(Engine& E) {
     E.gexec = nullptr;
     return E.fail_cuda("cudaGraphInstantiate", ei);
   }
+  // upload now, so that the first launch of a run does not carry it
+  CK(cudaGraphUpload(E.gexec, E.own));
+  CK(cudaStreamSynchronize(E.own));
   return ESC_OK;
 }
 
@@ -840,6 +843,11 @@ esc_status adjoint_graph(Engine& E, int kind, int buf, int len, cudaGraphExec_t*
   const cudaError_t ei = cudaGraphInstantiate(&ex, graph, 0);
   cudaGraphDestroy(graph);
   if (ei != cudaSuccess) return E.fail_cuda("cudaGraphInstantiate", ei);
+  const cudaError_t eu = cudaGraphUpload(ex, E.own);
+  if (eu != cudaSuccess) {
+    cudaGraphExecDestroy(ex);
+    return E.fail_cuda("cudaGraphUpload", eu);
+  }
   A.graphs[key] = ex;
   *out = ex;
   return ESC_OK;
