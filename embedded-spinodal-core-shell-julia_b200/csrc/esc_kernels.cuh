@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
   __shared__ double red[32];
   __shared__ int lastflag;
   const InstDev& I = insts[blockIdx.y];
-  if (*I.status) return;
+  const int status = *(volatile const int*)I.status;  // read after the column loads are issued
   const int w = threadIdx.x % W, t = threadIdx.x / W;
   const int kx = blockIdx.x * W + w;
   const bool active = kx < H;
@@ -453,6 +453,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = active ? ldc(S + (size_t)(t + T * m) * H + kx) : mkc<SR>(0, 0);
   }
+  if (status) return;  // block-uniform: one instance per block
   cpx<SR>* sms = reinterpret_cast<cpx<SR>*>(smraw);
   fft<false, P>(v, t, sms, lay, PassTable<P, SR>{});
 
@@ -629,7 +630,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];
   const InstDev& I = insts[blockIdx.y];
-  if (*I.status) return;
+  const int status = *(volatile const int*)I.status;  // read after the column loads are issued
   const int w = threadIdx.x % W, t = threadIdx.x / W;
   const int kx = blockIdx.x * W + w;
   const bool active = kx < H;
@@ -648,6 +649,7 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b
       b[m] = mkc<WR>(0, 0);
     }
   }
+  if (status) return;  // block-uniform: one instance per block
   cpx<WR>* smw = reinterpret_cast<cpx<WR>*>(smraw);
   if constexpr (kSplitMixed<SR, WR>) {
     // both flux components in one packed transform (lane 0: x, lane 1: y)

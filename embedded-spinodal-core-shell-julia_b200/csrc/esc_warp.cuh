@@ -159,6 +159,15 @@ __device__ __forceinline__ bool warp_instance_running(const int* status) {
   if ((threadIdx.x & 31) == 0) s = *(volatile const int*)status;
   return __shfl_sync(0xffffffffu, s, 0) == 0;
 }
+// The same test split in two: the status load is issued first and read after
+// the row loads, so a warp waits for one memory round trip instead of two.  A
+// stopped instance's rows are still valid memory; they are loaded and dropped.
+__device__ __forceinline__ int warp_status_issue(const int* status) {
+  int s = 0;
+  if ((threadIdx.x & 31) == 0) s = *(volatile const int*)status;
+  return s;
+}
+__device__ __forceinline__ bool warp_status_running(int s) { return __shfl_sync(0xffffffffu, s, 0) == 0; }
 
 // =====================================================================================
 template <class P, typename SR, typename WR>
@@ -169,7 +178,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   constexpr int tiles = WG::tiles_pairs;
   extern __shared__ __align__(16) unsigned char smraw[];
   const InstDev& I = insts[blockIdx.y];
-  if (!warp_instance_running(I.status)) return;
+  const int status = warp_status_issue(I.status);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = WG::thread_in_group(), gw = WG::group_in_warp();  // thread and group inside the warp
   const int g = WG::group_in_block();                               // group inside the block
@@ -191,6 +200,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = mkc<SR>(0, 0);
   }
+  if (!warp_status_running(status)) return;
   cpx<SR>* xs = reinterpret_cast<cpx<SR>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<SR>)> lay_s{g * N, gw};
   fft<true, P, typename WG::Sync>(v, t, xs, lay_s, PassTable<P, SR>{});
@@ -301,7 +311,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   constexpr int tiles = WG::tiles_rows;
   extern __shared__ __align__(16) unsigned char smraw[];
   const InstDev& I = insts[blockIdx.y];
-  if (!warp_instance_running(I.status)) return;
+  const int status = warp_status_issue(I.status);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = WG::thread_in_group(), gw = WG::group_in_warp();
   const int g = WG::group_in_block();
@@ -320,6 +330,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = mkc<WR>(0, 0);
   }
+  if (!warp_status_running(status)) return;
   cpx<WR>* xw = reinterpret_cast<cpx<WR>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<WR>)> lay{g * N, gw};
   fft<true, P, typename WG::Sync>(v, t, xw, lay, PassTable<P, WR>{});
@@ -435,7 +446,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
   constexpr int tiles = WG::tiles_pairs;
   extern __shared__ __align__(16) unsigned char smraw[];
   const InstDev& I = insts[blockIdx.y];
-  if (!warp_instance_running(I.status)) return;
+  const int status = warp_status_issue(I.status);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = WG::thread_in_group(), gw = WG::group_in_warp();
   const int g = WG::group_in_block();
@@ -457,6 +468,7 @@ __global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = mkc<f2>(f2(0.0f, 0.0f), f2(0.0f, 0.0f));
   }
+  if (!warp_status_running(status)) return;
   cpx<f2>* xs = reinterpret_cast<cpx<f2>*>(smraw);
   const SwizzleLayout<N, sizeof(cpx<f2>)> lay{g * N, gw};
   const PassTableDup<P> twp{};
