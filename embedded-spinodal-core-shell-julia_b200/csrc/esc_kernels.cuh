@@ -238,6 +238,9 @@ __device__ __forceinline__ void prefetch_l1(const void* p, int bytes, int t, int
   for (int l = t; l * 128 < bytes; l += nthr) asm volatile("prefetch.global.L1 [%0];" ::"l"(c + 128 * l));
 }
 
+// L2 prefetch of the 128-byte line holding `p`
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 template <typename R>
 __device__ __forceinline__ R mobility_of(R phi, R M0) {
   return M0 * (phi * phi * phi * ((R)10 - (R)15 * phi + (R)6 * phi * phi));
@@ -454,6 +457,12 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a
     for (int m = 0; m < E; ++m) v[m] = active ? ldc(S + (size_t)(t + T * m) * H + kx) : mkc<SR>(0, 0);
   }
   if (status) return;  // block-uniform: one instance per block
+  if (w == 0) {
+    // F is read after the S transform: start pulling this block's rows of it into L2
+    const cpx<WR>* F = reinterpret_cast<const cpx<WR>*>(I.F) + (size_t)blockIdx.x * W;
+#pragma unroll
+    for (int m = 0; m < E; ++m) prefetch_l2(F + (size_t)(t + T * m) * H);
+  }
   cpx<SR>* sms = reinterpret_cast<cpx<SR>*>(smraw);
   fft<false, P>(v, t, sms, lay, PassTable<P, SR>{});
 
@@ -650,6 +659,12 @@ __global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b
     }
   }
   if (status) return;  // block-uniform: one instance per block
+  if (w == 0) {
+    // S is updated after both transforms: start pulling this block's rows of it into L2
+    const cpx<SR>* S = reinterpret_cast<const cpx<SR>*>(I.S) + (size_t)blockIdx.x * W;
+#pragma unroll
+    for (int m = 0; m < E; ++m) prefetch_l2(S + (size_t)(t + T * m) * H);
+  }
   cpx<WR>* smw = reinterpret_cast<cpx<WR>*>(smraw);
   if constexpr (kSplitMixed<SR, WR>) {
     // both flux components in one packed transform (lane 0: x, lane 1: y)
