@@ -399,7 +399,9 @@ def main():
     ms_mixed = max_over_ranks(ms_mixed)
     value = world * pts * args.steps / (ms_mixed / 1000.0)
     n_groups = len(set(ns))
-    gpu_launches = n_groups * (1 + 4 * args.steps + 3 + 1) + (args.steps // 32) + (1 if args.steps % 32 else 0)
+    # per size group: init, 4 phases per step, the final history row (3), fin, and one step-counter
+    # advance per captured 32-step chunk and per remainder
+    gpu_launches = n_groups * (1 + 4 * args.steps + 3 + 1 + args.steps // 32 + (1 if args.steps % 32 else 0))
 
     # roofline of the dominant kernel: per-phase CUDA-event timing on the same batch
     prof = bm.profile_phases(steps=5)

@@ -11,12 +11,15 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "esc.h"
@@ -73,6 +76,8 @@ struct Group {
   unsigned* cnt = nullptr;
   int* status = nullptr;
   long long* bad = nullptr;
+  int* base = nullptr;               // this group's step counter (history row of its next step)
+  cudaGraphExec_t gexec = nullptr;   // kChunk steps of this group, captured on its own stream
   esc::InstDev* d_inst = nullptr;
   std::vector<esc::InstDev> h_inst;
   esc::ColMaps maps;      // tensor maps of S, F, G for the pipelined column kernels
@@ -155,9 +160,8 @@ struct Engine {
   int* base = nullptr;
   double* hist = nullptr;
   size_t hist_cap = 0;  // doubles
-  cudaGraphExec_t gexec = nullptr;
-  std::vector<cudaStream_t> side;    // per-group capture streams
-  std::vector<cudaEvent_t> side_ev;  // per-group join events
+  std::vector<cudaStream_t> side;    // per-group streams (their graphs, copies and tails)
+  std::vector<cudaEvent_t> side_ev;  // per-group completion / join events
   cudaEvent_t fork_ev = nullptr;
   std::vector<void*> allocs;
   std::string err;
@@ -207,8 +211,10 @@ struct Engine {
   }
 
   void release() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    gexec = nullptr;
+    for (Group& g : groups) {
+      if (g.gexec) cudaGraphExecDestroy(g.gexec);
+      g.gexec = nullptr;
+    }
     for (auto& kv : adj.graphs) cudaGraphExecDestroy(kv.second);
     adj.graphs.clear();
     for (int b = 0; b < 2; ++b) {
@@ -332,6 +338,7 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
     TRY(E.alloc(&g.cnt, cnt * 4 * sizeof(unsigned), "counters"));
     TRY(E.alloc(&g.status, cnt * sizeof(int), "status"));
     TRY(E.alloc(&g.bad, cnt * sizeof(long long), "bad step"));
+    TRY(E.alloc(&g.base, sizeof(int), "step counter"));
     TRY(E.alloc(&g.d_inst, cnt * sizeof(esc::InstDev), "descriptors"));
     // twiddles
     if (sr == 8) {
@@ -629,17 +636,28 @@ void launch_step(Engine& E, int s_local, cudaStream_t st) {
   }
 }
 
+// Each size group advances on its own stream: a captured graph of kChunk steps
+// of that group with its own step counter.  The groups' chains are independent
+// (one instance never reads another), so they overlap on the GPU and fill each
+// other's launch tails, and in a run with host buffers one group's copies
+// overlap the other groups' steps.
 esc_status ensure_graph(Engine& E) {
-  if (E.gexec) return ESC_OK;
-  cudaGraph_t graph = nullptr;
-  // The size groups are independent for a whole chunk: each group's chain of
-  // kChunk steps is captured on its own forked stream, so the chains overlap and
-  // fill each other's launch tails; they join before the step counter advances.
   const int ng = (int)E.groups.size();
   if ((int)E.side.size() < ng) {
+    // stream priority by work: the group with the most points gets the highest
+    // priority, so it finishes first and its D2H copies overlap the rest
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     for (int i = (int)E.side.size(); i < ng; ++i) {
+      const double work = (double)E.groups[i].members.size() * E.groups[i].n * E.groups[i].n;
+      int rank = 0;
+      for (int j = 0; j < ng; ++j) {
+        const double wj = (double)E.groups[j].members.size() * E.groups[j].n * E.groups[j].n;
+        if (wj > work || (wj == work && j < i)) ++rank;
+      }
+      const int prio = std::min(least, greatest + rank);
       cudaStream_t s = nullptr;
-      CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio));
       E.side.push_back(s);
       cudaEvent_t ev = nullptr;
       CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -647,41 +665,34 @@ esc_status ensure_graph(Engine& E) {
     }
     if (!E.fork_ev) CK(cudaEventCreateWithFlags(&E.fork_ev, cudaEventDisableTiming));
   }
-  const char* fork_env = getenv("ESC_GRAPH_FORK");
-  const bool fork = !(fork_env && fork_env[0] == '0') && ng > 1;
-  CK(cudaStreamBeginCapture(E.own, cudaStreamCaptureModeThreadLocal));
-  if (!fork) {
-    for (int s = 0; s < kChunk; ++s) launch_step(E, s, E.own);
-  }
-  CK(cudaEventRecord(E.fork_ev, E.own));
-  for (int gi = 0; fork && gi < ng; ++gi) {
-    cudaStream_t ss = E.side[gi];
-    CK(cudaStreamWaitEvent(ss, E.fork_ev, 0));
+  for (int gi = 0; gi < ng; ++gi) {
     Group& g = E.groups[gi];
+    if (g.gexec) continue;
+    cudaStream_t ss = E.side[gi];
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(ss, cudaStreamCaptureModeThreadLocal));
     for (int s = 0; s < kChunk; ++s) {
-      phase_row_a(g, E.base, s, ss);
-      phase_col_a(g, E.base, s, ss);
-      phase_row_b(g, E.base, s, ss);
+      phase_row_a(g, g.base, s, ss);
+      phase_col_a(g, g.base, s, ss);
+      phase_row_b(g, g.base, s, ss);
       phase_col_b(g, ss);
     }
-    CK(cudaEventRecord(E.side_ev[gi], ss));
-    CK(cudaStreamWaitEvent(E.own, E.side_ev[gi], 0));
+    k_advance<<<1, 32, 0, ss>>>(g.base, kChunk);
+    const cudaError_t ec = cudaStreamEndCapture(ss, &graph);
+    if (ec != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return E.fail_cuda("cudaStreamEndCapture", ec);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&g.gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      g.gexec = nullptr;
+      return E.fail_cuda("cudaGraphInstantiate", ei);
+    }
+    // upload now, so that the first launch of a run does not carry it
+    CK(cudaGraphUpload(g.gexec, ss));
+    CK(cudaStreamSynchronize(ss));
   }
-  k_advance<<<1, 32, 0, E.own>>>(E.base, kChunk);
-  const cudaError_t ec = cudaStreamEndCapture(E.own, &graph);
-  if (ec != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    return E.fail_cuda("cudaStreamEndCapture", ec);
-  }
-  const cudaError_t ei = cudaGraphInstantiate(&E.gexec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (ei != cudaSuccess) {
-    E.gexec = nullptr;
-    return E.fail_cuda("cudaGraphInstantiate", ei);
-  }
-  // upload now, so that the first launch of a run does not carry it
-  CK(cudaGraphUpload(E.gexec, E.own));
-  CK(cudaStreamSynchronize(E.own));
   return ESC_OK;
 }
 
@@ -730,69 +741,105 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
     }
     CK(cudaMemcpyAsync(g.d_inst, g.h_inst.data(), g.h_inst.size() * sizeof(esc::InstDev),
                        cudaMemcpyHostToDevice, st));
-    if (!device_io) {
-      for (size_t s = 0; s < g.members.size(); ++s)
-        CK(cudaMemcpyAsync(g.cio + s * nn, cptr[g.members[s]], nn * sizeof(double), cudaMemcpyHostToDevice, st));
-    }
     CK(cudaMemsetAsync(g.status, 0, g.members.size() * sizeof(int), st));
     CK(cudaMemsetAsync(g.bad, 0xff, g.members.size() * sizeof(long long), st));
     CK(cudaMemsetAsync(g.cnt, 0, g.members.size() * 4 * sizeof(unsigned), st));
+    CK(cudaMemsetAsync(g.base, 0, sizeof(int), st));
   }
-  CK(cudaMemsetAsync(E.base, 0, sizeof(int), st));
-  for (Group& g : E.groups) g.ks->init(g.d_inst, (int)g.members.size(), st);
-  CK(cudaGetLastError());
-  int done = 0;
-  if (steps >= kChunk) {
-    TRY(ensure_graph(E));
-    while (steps - done >= kChunk) {
-      CK(cudaGraphLaunch(E.gexec, st));
-      done += kChunk;
+  TRY(ensure_graph(E));
+  // Every group runs on its own stream, forked from (and joined back into) the
+  // caller's stream: H2D of its fields, the steps, the final history row, and
+  // (below) its D2H copies.  The smallest groups are queued first, so that
+  // steps start while the larger fields are still being copied in; the
+  // largest group has the highest stream priority and finishes first.
+  const int ng = (int)E.groups.size();
+  std::vector<int> order(ng);
+  for (int gi = 0; gi < ng; ++gi) order[gi] = gi;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const Group &ga = E.groups[a], &gb = E.groups[b];
+    return (double)ga.members.size() * ga.n * ga.n < (double)gb.members.size() * gb.n * gb.n;
+  });
+  CK(cudaEventRecord(E.fork_ev, st));
+  for (int gi : order) {
+    Group& g = E.groups[gi];
+    cudaStream_t ss = E.side[gi];
+    const int cnt = (int)g.members.size();
+    const size_t nn = (size_t)g.n * g.n;
+    CK(cudaStreamWaitEvent(ss, E.fork_ev, 0));
+    if (!device_io) {
+      for (int s = 0; s < cnt; ++s)
+        CK(cudaMemcpyAsync(g.cio + s * nn, cptr[g.members[s]], nn * sizeof(double), cudaMemcpyHostToDevice, ss));
     }
+    g.ks->init(g.d_inst, cnt, ss);
+    int done = 0;
+    for (; steps - done >= kChunk; done += kChunk) CK(cudaGraphLaunch(g.gexec, ss));
+    const int rem = steps - done;
+    for (int s = 0; s < rem; ++s) {
+      phase_row_a(g, g.base, s, ss);
+      phase_col_a(g, g.base, s, ss);
+      phase_row_b(g, g.base, s, ss);
+      phase_col_b(g, ss);
+    }
+    if (rem) k_advance<<<1, 32, 0, ss>>>(g.base, rem);
+    // history row `steps` of the final field (no update)
+    phase_row_a(g, g.base, 0, ss);
+    phase_col_a(g, g.base, 0, ss);
+    phase_row_b(g, g.base, 0, ss);
+    g.ks->fin(g.d_inst, cnt, ss);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(E.side_ev[gi], ss));
   }
-  const int rem = steps - done;
-  for (int s = 0; s < rem; ++s) launch_step(E, s, st);
-  if (rem) k_advance<<<1, 32, 0, st>>>(E.base, rem);
-  // history row `steps` of the final field (no update)
-  for (Group& g : E.groups) {
-    phase_row_a(g, E.base, 0, st);
-    phase_col_a(g, E.base, 0, st);
-    phase_row_b(g, E.base, 0, st);
-  }
-  for (Group& g : E.groups) g.ks->fin(g.d_inst, (int)g.members.size(), st);
-  CK(cudaGetLastError());
-  // statuses
+  // As each group finishes: read its statuses, then queue its D2H copies on its
+  // stream, beside the groups still stepping; the caller's stream joins them.
   std::vector<int> status(E.count, 0);
   std::vector<long long> bad(E.count, -1);
-  for (Group& g : E.groups) {
-    std::vector<int> s(g.members.size());
-    std::vector<long long> b(g.members.size());
-    CK(cudaMemcpyAsync(s.data(), g.status, s.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(b.data(), g.bad, b.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (size_t k = 0; k < g.members.size(); ++k) {
-      status[g.members[k]] = s[k];
-      bad[g.members[k]] = b[k];
+  std::vector<char> pending(ng, 1);
+  for (int left = ng; left > 0;) {
+    bool progressed = false;
+    for (int gi : order) {
+      if (!pending[gi]) continue;
+      const cudaError_t q = cudaEventQuery(E.side_ev[gi]);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) return E.fail_cuda("cudaEventQuery", q);
+      Group& g = E.groups[gi];
+      cudaStream_t ss = E.side[gi];
+      const size_t cnt = g.members.size(), nn = (size_t)g.n * g.n;
+      std::vector<int> sg(cnt);
+      std::vector<long long> bg(cnt);
+      CK(cudaMemcpyAsync(sg.data(), g.status, cnt * sizeof(int), cudaMemcpyDeviceToHost, ss));
+      CK(cudaMemcpyAsync(bg.data(), g.bad, cnt * sizeof(long long), cudaMemcpyDeviceToHost, ss));
+      CK(cudaStreamSynchronize(ss));
+      for (size_t k = 0; k < cnt; ++k) {
+        status[g.members[k]] = sg[k];
+        bad[g.members[k]] = bg[k];
+      }
+      if (!device_io) {
+        for (size_t k = 0; k < cnt; ++k) {
+          const int i = g.members[k];
+          if (status[i] && leave_bad_unchanged) continue;
+          CK(cudaMemcpyAsync(cptr[i], g.cio + k * nn, nn * sizeof(double), cudaMemcpyDeviceToHost, ss));
+        }
+      }
+      if (hist_host) {
+        for (size_t k = 0; k < cnt; ++k) {
+          const int i = g.members[k];
+          if (hist_host[i])
+            CK(cudaMemcpyAsync(hist_host[i], hbase + (size_t)i * per, per * sizeof(double), cudaMemcpyDeviceToHost,
+                               ss));
+        }
+      }
+      CK(cudaEventRecord(E.side_ev[gi], ss));
+      CK(cudaStreamWaitEvent(st, E.side_ev[gi], 0));
+      pending[gi] = 0;
+      --left;
+      progressed = true;
     }
+    if (!progressed && left > 0) std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
   bool any_bad = false;
   for (int i = 0; i < E.count; ++i) {
     if (status[i]) any_bad = true;
     if (bad_out) bad_out[i] = status[i] ? (int64_t)bad[i] : -1;
-  }
-  if (!device_io) {
-    for (Group& g : E.groups) {
-      const size_t nn = (size_t)g.n * g.n;
-      for (size_t s = 0; s < g.members.size(); ++s) {
-        const int i = g.members[s];
-        if (status[i] && leave_bad_unchanged) continue;
-        CK(cudaMemcpyAsync(cptr[i], g.cio + s * nn, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
-      }
-    }
-  }
-  if (hist_host) {
-    for (int i = 0; i < E.count; ++i)
-      if (hist_host[i])
-        CK(cudaMemcpyAsync(hist_host[i], hbase + (size_t)i * per, per * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
   CK(cudaStreamSynchronize(st));
   if (any_bad) {
