@@ -100,6 +100,14 @@ struct KS {
     const size_t el = row > col ? row : col;
     return el * sizeof(cpx<SR>);
   }
+  // forward column kernels (ColGeomF: col_block<P>() threads, CW columns per block)
+  static constexpr int CB = ColGeomF<P, SR, WR>::B, CW = ColGeomF<P, SR, WR>::W;
+  static constexpr int ctiles = (H + CW - 1) / CW;
+  static size_t col_smem() {
+    const size_t col = (size_t)host_smpad(N * CW - 1) + 1;
+    const size_t row = (size_t)G * RowLayout<N>::stride;
+    return (row > col ? row : col) * sizeof(cpx<SR>);
+  }
   static cudaError_t prepare() {
     const int bytes = (int)smem();
     cudaError_t e;
@@ -107,11 +115,11 @@ struct KS {
     if ((e = cudaFuncSetAttribute(k_final<P, SR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
     if ((e = cudaFuncSetAttribute(k_row_a<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
       return e;
-    if ((e = cudaFuncSetAttribute(k_col_a<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
+    if ((e = cudaFuncSetAttribute(k_col_a<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem())))
       return e;
     if ((e = cudaFuncSetAttribute(k_row_b<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
       return e;
-    if ((e = cudaFuncSetAttribute(k_col_b<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
+    if ((e = cudaFuncSetAttribute(k_col_b<P, SR, WR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem())))
       return e;
     return prepare_alt();
   }
@@ -125,13 +133,13 @@ struct KS {
     k_row_a<P, SR, WR><<<dim3(tiles_pairs, count), kBlock, smem(), st>>>(d, base, s);
   }
   static void col_a(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
-    k_col_a<P, SR, WR><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(d, base, s);
+    k_col_a<P, SR, WR><<<dim3(ctiles, count), CB, col_smem(), st>>>(d, base, s);
   }
   static void row_b(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
     k_row_b<P, SR, WR><<<dim3(tiles_rows, count), kBlock, smem(), st>>>(d, base, s);
   }
   static void col_b(const InstDev* d, int count, cudaStream_t st) {
-    k_col_b<P, SR, WR><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(d);
+    k_col_b<P, SR, WR><<<dim3(ctiles, count), CB, col_smem(), st>>>(d);
   }
   using PG = PipeGeom<P, SR, WR>;
   // occupancy (blocks per SM) of the persistent kernels and the SM count, set by prepare()
@@ -215,7 +223,7 @@ struct KS {
   using WP = typename WarpPlan<N>::type;    // row B (and the adjoint's row B)
   template <class Q>
   static constexpr bool group_ok() {
-    return ((Q::T <= 32) && (32 % Q::T == 0)) || Q::T == 64;
+    return ((Q::T <= 32) && (32 % Q::T == 0)) || Q::T == 64 || Q::T == 128 || Q::T == 256;
   }
   static constexpr bool warp_ok = group_ok<WPA>() && group_ok<WP>();
   static size_t warp_smem_a() {
@@ -262,9 +270,9 @@ struct KS {
   }
   // ---- alternative column plan ----
   using AP = typename AltPlan<N>::type;
-  static constexpr int alt_tiles_cols = (H + kBlock / AP::T - 1) / (kBlock / AP::T);
+  static constexpr int alt_tiles_cols = (H + ColGeomF<AP, SR, WR>::W - 1) / ColGeomF<AP, SR, WR>::W;
   static size_t alt_smem() {
-    constexpr int Ga = kBlock / AP::T, Wa = kBlock / AP::T;
+    constexpr int Ga = kBlock / AP::T, Wa = ColGeomF<AP, SR, WR>::W;
     const size_t row = (size_t)Ga * RowLayout<N>::stride;
     const size_t col = (size_t)host_smpad(N * Wa - 1) + 1;
     return (row > col ? row : col) * sizeof(cpx<SR>);
@@ -277,10 +285,10 @@ struct KS {
     return cudaSuccess;
   }
   static void col_a_alt(const InstDev* d, int count, const int* base, int s, cudaStream_t st) {
-    k_col_a<AP, SR, WR><<<dim3(alt_tiles_cols, count), kBlock, alt_smem(), st>>>(d, base, s);
+    k_col_a<AP, SR, WR><<<dim3(alt_tiles_cols, count), ColGeomF<AP, SR, WR>::B, alt_smem(), st>>>(d, base, s);
   }
   static void col_b_alt(const InstDev* d, int count, cudaStream_t st) {
-    k_col_b<AP, SR, WR><<<dim3(alt_tiles_cols, count), kBlock, alt_smem(), st>>>(d);
+    k_col_b<AP, SR, WR><<<dim3(alt_tiles_cols, count), ColGeomF<AP, SR, WR>::B, alt_smem(), st>>>(d);
   }
   // ---- pass-major twiddle tables ----
   template <class Q, typename Re>

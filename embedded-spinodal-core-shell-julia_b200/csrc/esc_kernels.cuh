@@ -265,9 +265,23 @@ struct ColGeom {
 // precision's transforms fit 3 blocks at up to 8 elements per thread and 2 at
 // up to 16; the FP64 drop-in fits 2 at up to 8; larger plans keep the
 // compiler's choice.
+// Block size of the forward column kernels: 256 threads, or, in the mixed
+// precision, two columns for plans of 256 threads per column (n = 4096), where
+// one column per block reads 16-byte halves of 32-byte sectors.  (The FP64
+// transforms need more than the 128 registers a 512-thread block leaves.)
+template <class P, typename SR, typename WR>
+constexpr int col_block() {
+  return (kSplitMixed<SR, WR> && P::T >= 256) ? 2 * P::T : kBlock;
+}
+template <class P, typename SR, typename WR>
+struct ColGeomF {
+  static constexpr int B = col_block<P, SR, WR>();
+  static constexpr int W = B / P::T;
+};
 template <class P, typename SR, typename WR>
 constexpr int col_min_blocks() {
-  return kSplitMixed<SR, WR> ? (P::E <= 8 ? 3 : (P::E <= 16 ? 2 : 1)) : (P::E <= 8 ? 2 : 1);
+  constexpr int b256 = kSplitMixed<SR, WR> ? (P::E <= 8 ? 3 : (P::E <= 16 ? 2 : 1)) : (P::E <= 8 ? 2 : 1);
+  return b256 * kBlock / col_block<P, SR, WR>() > 1 ? b256 * kBlock / col_block<P, SR, WR>() : 1;
 }
 
 // init: c (FP64 real) -> S (packed x-transform), one row pair per group
@@ -434,9 +448,9 @@ __global__ void __launch_bounds__(kBlock) k_row_a(const InstDev* __restrict__ in
 
 // col A: y-FFT of S and F, gradient energy, mu^, inverse y-FFT of i k mu^ -> G
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_a(const InstDev* __restrict__ insts, const int* __restrict__ base,
+__global__ void __launch_bounds__(col_block<P, SR, WR>(), (col_min_blocks<P, SR, WR>())) k_col_a(const InstDev* __restrict__ insts, const int* __restrict__ base,
                                                   int s_local) {
-  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeomF<P, SR, WR>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];
   __shared__ int lastflag;
@@ -634,8 +648,8 @@ __global__ void __launch_bounds__(kBlock) k_row_b(const InstDev* __restrict__ in
 
 // col B: y-FFT of the fluxes, divergence, stabilised increment, inverse y-FFT, S += increment
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(kBlock, (col_min_blocks<P, SR, WR>())) k_col_b(const InstDev* __restrict__ insts) {
-  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
+__global__ void __launch_bounds__(col_block<P, SR, WR>(), (col_min_blocks<P, SR, WR>())) k_col_b(const InstDev* __restrict__ insts) {
+  constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeomF<P, SR, WR>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32];
   const InstDev& I = insts[blockIdx.y];

@@ -50,15 +50,18 @@ constexpr int kWarpBlock = ESC_WARP_BLOCK;
 constexpr int kWarpBlocksPerSM = 512 / kWarpBlock;  // 16 warps per SM at up to 128 registers
 
 // Groups of T <= 32 threads live inside one warp (one-warp blocks, __syncwarp).
-// Groups of 64 threads are a whole two-warp block (__syncthreads): E8 plans of
-// the larger sizes, with half the registers per thread of the E16 plans.
+// Larger groups (64 to 256 threads) are a whole block (__syncthreads): E8 plans
+// of the mid sizes, with half the registers per thread of the E16 plans, and
+// the E16 plans of n >= 2048.
 template <class P>
 struct WarpRowGeom {
   static constexpr int N = P::N, T = P::T, H = N / 2;
   static constexpr bool kInWarp = T <= 32;
-  static_assert((kInWarp && 32 % T == 0) || T == 64, "groups inside one warp, or a 64-thread block");
+  static_assert((kInWarp && 32 % T == 0) || T == 64 || T == 128 || T == 256,
+                "groups inside one warp, or a block of 64, 128 or 256 threads");
   static constexpr int BLOCK = kInWarp ? kWarpBlock : T;  // threads per block
-  static constexpr int MINB = kInWarp ? kWarpBlocksPerSM : (P::E <= 8 ? 12 : 8);  // blocks per SM compiled for
+  // blocks per SM compiled for: 128 registers per thread for T >= 128
+  static constexpr int MINB = kInWarp ? kWarpBlocksPerSM : (T == 64 ? (P::E <= 8 ? 12 : 8) : 512 / T);
   static constexpr int GPW = kInWarp ? 32 / T : 1;        // groups per warp
   static constexpr int NW = BLOCK / 32;                   // warps per block
   static constexpr int G = kInWarp ? GPW * NW : 1;        // groups per block

@@ -71,3 +71,48 @@ def test_mixed_default_example_error_bound():
     c32, h32 = esc.run_simulation(c0, phi, dt=0.01, steps=1000, precision="mixed")
     assert np.max(np.abs(c32 - c64)) < 1e-5
     assert np.max(np.abs(h32[:, 1] - c0.mean())) < 1e-12
+
+
+_LARGE_ORACLE = {}
+
+
+def _large_oracle(n, steps):
+    """Oracle run of the large-grid case (computed once per session; a few seconds each)."""
+    key = (n, steps)
+    if key not in _LARGE_ORACLE:
+        import os
+        orc.set_workers(os.cpu_count() or 1)
+        c0, phi = case(n)
+        _LARGE_ORACLE[key] = (c0, phi) + orc.run_simulation(c0, phi, dt=0.01, steps=steps)
+    return _LARGE_ORACLE[key]
+
+
+@pytest.mark.parametrize("n,steps", [(1536, 2), (2048, 2), (3072, 1), (4096, 1)])
+def test_fp64_matches_oracle_large(n, steps):
+    """The sizes whose row transforms run in groups of 128 or 256 threads (a whole block)."""
+    c0, phi, co, ho = _large_oracle(n, steps)
+    c, h = esc.run_simulation(c0, phi, dt=0.01, steps=steps)
+    assert rel(c, co) < RTOL_FP64
+    assert max(hist_rel(h, ho)) < RTOL_FP64
+
+
+@pytest.mark.parametrize("rows", ["legacy", "pipe", "warp"])
+def test_fp64_row_families_large(rows, monkeypatch):
+    """Every row-kernel family at n = 2048 (the tuner chooses among them) against the oracle."""
+    monkeypatch.setenv("ESC_ROWS", rows)
+    c0, phi, co, ho = _large_oracle(2048, 2)
+    c, h = esc.run_simulation(c0, phi, dt=0.01, steps=2)
+    assert rel(c, co) < RTOL_FP64
+    assert max(hist_rel(h, ho)) < RTOL_FP64
+
+
+@pytest.mark.parametrize("n", [2048, 4096])
+def test_mixed_large_against_fp64(n):
+    """Mixed precision at the large sizes (packed two-row transforms in 256-thread groups,
+    two-column blocks at n = 4096) stays within its bound of the FP64 result and conserves mass."""
+    c0, phi = case(n)
+    c64, h64 = esc.run_simulation(c0, phi, dt=0.01, steps=20)
+    c32, h32 = esc.run_simulation(c0, phi, dt=0.01, steps=20, precision="mixed")
+    assert rel(c32, c64) < 1e-5
+    assert np.max(np.abs(h32[:, 1] - h32[0, 1])) < 1e-12
+    assert np.max(np.abs(h32[:, 2] - h64[:, 2])) / np.max(np.abs(h64[:, 2])) < 1e-5
