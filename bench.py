@@ -378,14 +378,16 @@ def main():
         stream = torch.cuda.current_stream()
         b.set_stream(stream.cuda_stream)
         work = [c.clone() for c in dc0]
-        b.run_device([w.data_ptr() for w in work], warmup, DT)
-        for w, c in zip(work, dc0):
-            w.copy_(c)
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # the sampler starts before the warm-up, so that its start-up pause does not
+        # leave the GPU idle between the warm-up and the timed steps
         with ClockSampler(local) as clk:
+            b.run_device([w.data_ptr() for w in work], warmup, DT)
+            for w, c in zip(work, dc0):
+                w.copy_(c)
+            torch.cuda.synchronize()
+            barrier()
+            torch.cuda.synchronize()
             ev0.record(stream)
             bads = b.run_device([w.data_ptr() for w in work], steps, DT)
             ev1.record(stream)

@@ -51,24 +51,68 @@ __device__ __forceinline__ R fpp_of(R c, R phi, const ModelParams& p) {
 }
 __device__ __forceinline__ double gphi_of(double phi) { return phi * phi * (1.0 - phi) * (1.0 - phi); }
 
+// block_reduce<OpSum> of NV values at once (same shuffle trees, same bits); red
+// holds 32 doubles per value
+template <int NV>
+__device__ __forceinline__ void block_reduce_n(double (&v)[NV], double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) red[32 * q + wid] = v[q];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      v[q] = (lane < (int)(blockDim.x >> 5)) ? red[32 * q + lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) red[32 * q] = v[q];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = red[32 * q];
+  __syncthreads();
+}
+
 // fold this block's values into acc[slot..] once every block has arrived
 template <int NV>
 __device__ __forceinline__ void adj_accumulate(const AdjDev& A, int counter, int part_off, const double (&v)[NV],
                                                const int (&slot)[NV], double* red, int* flag) {
   double r[NV];
 #pragma unroll
-  for (int q = 0; q < NV; ++q) r[q] = block_reduce<OpSum>(v[q], red);
+  for (int q = 0; q < NV; ++q) r[q] = v[q];
+  block_reduce_n(r, red);
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) A.part[part_off + (size_t)blockIdx.x * NV + q] = r[q];
   }
   if (!arrive_last(&A.cnt[counter], gridDim.x, flag)) return;
+  // the NV folds of reduce_partials, in one pass (same order, same bits)
+  double tot[NV];
 #pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    const double tot = reduce_partials<OpSum>(A.part + part_off + q, gridDim.x, NV, 0.0, red);
-    if (threadIdx.x == 0) A.acc[slot[q]] += tot;
+  for (int q = 0; q < NV; ++q) tot[q] = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) tot[q] += __ldcg(A.part + part_off + (size_t)i * NV + q);
   }
-  if (threadIdx.x == 0) A.cnt[counter] = 0;
+  block_reduce_n(tot, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) A.acc[slot[q]] += tot[q];
+    A.cnt[counter] = 0;
+  }
 }
 
 // ---- column 1 -------------------------------------------------------------------------
@@ -76,7 +120,7 @@ template <class P>
 __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col1(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double red[32];
+  __shared__ double red[32 * 4];
   __shared__ int lastflag;
   const AdjDev& A = adjs[blockIdx.y];
   const int w = threadIdx.x % W, t = threadIdx.x / W;
@@ -84,7 +128,7 @@ __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col1(const 
   const bool active = kx < H;
   const ColLayout<W> lay{w};
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const cpx<double>* tw = reinterpret_cast<const cpx<double>*>(A.tw);
+  const PassTable<P, double> tw{};  // pass-major copy of the FP64 table A.tw
   const double kunit = 2.0 * 3.14159265358979323846 / ((double)N * A.dx);
   const double c1 = 2.0 * A.p.Q * A.p.kappa * A.dt;
   cpx<double> l[E], d[E];
@@ -189,7 +233,7 @@ template <class P>
 __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col2(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double red[32];
+  __shared__ double red[32 * 4];
   __shared__ int lastflag;
   const AdjDev& A = adjs[blockIdx.y];
   const int w = threadIdx.x % W, t = threadIdx.x / W;
@@ -197,7 +241,7 @@ __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col2(const 
   const bool active = kx < H;
   const ColLayout<W> lay{w};
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const cpx<double>* tw = reinterpret_cast<const cpx<double>*>(A.tw);
+  const PassTable<P, double> tw{};  // pass-major copy of the FP64 table A.tw
   const double kunit = 2.0 * 3.14159265358979323846 / ((double)N * A.dx);
   cpx<double> fx[E], fy[E];
 #pragma unroll
@@ -302,7 +346,7 @@ template <class P>
 __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_row2(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, G = RowGeom<P>::G;
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double red[32];
+  __shared__ double red[32 * 4];
   __shared__ int lastflag;
   const AdjDev& A = adjs[blockIdx.y];
   const int t = threadIdx.x % T, g = threadIdx.x / T;
@@ -311,7 +355,7 @@ __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_row2(const 
   const int ya = 2 * pair;
   const RowLayout<N> lay{g * RowLayout<N>::stride};
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const cpx<double>* tw = reinterpret_cast<const cpx<double>*>(A.tw);
+  const PassTable<P, double> tw{};  // pass-major copy of the FP64 table A.tw
   const cpx<double>* Xg = reinterpret_cast<const cpx<double>*>(A.Xg);
   const cpx<double>* S = reinterpret_cast<const cpx<double>*>(A.S0);
   cpx<double> gv[E], cv[E];
@@ -370,7 +414,7 @@ __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_mu_col(cons
   const bool active = kx < H;
   const ColLayout<W> lay{w};
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const cpx<double>* tw = reinterpret_cast<const cpx<double>*>(A.tw);
+  const PassTable<P, double> tw{};  // pass-major copy of the FP64 table A.tw
   const double kunit = 2.0 * 3.14159265358979323846 / ((double)N * A.dx);
   const double kappa = A.p.kappa;
   cpx<double> v[E], f[E];
@@ -425,7 +469,7 @@ template <class P>
 __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_seed_row(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, G = RowGeom<P>::G;
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double red[32];
+  __shared__ double red[32 * 4];
   __shared__ int lastflag;
   const AdjDev& A = adjs[blockIdx.y];
   const int t = threadIdx.x % T, g = threadIdx.x / T;
@@ -434,7 +478,7 @@ __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_seed_row(co
   const int ya = 2 * pair;
   const RowLayout<N> lay{g * RowLayout<N>::stride};
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const cpx<double>* tw = reinterpret_cast<const cpx<double>*>(A.tw);
+  const PassTable<P, double> tw{};  // pass-major copy of the FP64 table A.tw
   const cpx<double>* Xm = reinterpret_cast<const cpx<double>*>(A.Xg);
   const cpx<double>* S = reinterpret_cast<const cpx<double>*>(A.S0);
   cpx<double> mv[E], cv[E];
