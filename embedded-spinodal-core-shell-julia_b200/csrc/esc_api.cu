@@ -1299,7 +1299,7 @@ esc_status esc_batch_run(esc_batch* b, double* const* c, int steps, double dt, d
     tl_err = "null batch";
     return ESC_EINVAL;
   }
-  return engine_run(b->e, c, false, steps, dt, history, nullptr, bad_steps, false);
+  return engine_run(b->e, c, false, steps, dt, history, nullptr, bad_steps, true);
 }
 
 esc_status esc_batch_run_device(esc_batch* b, double* const* c, int steps, double dt, double* history,
@@ -1308,7 +1308,7 @@ esc_status esc_batch_run_device(esc_batch* b, double* const* c, int steps, doubl
     tl_err = "null batch";
     return ESC_EINVAL;
   }
-  return engine_run(b->e, c, true, steps, dt, nullptr, history, bad_steps, false);
+  return engine_run(b->e, c, true, steps, dt, nullptr, history, bad_steps, true);
 }
 
 esc_status esc_batch_profile_phases(esc_batch* b, int steps, int* n_groups, int* group_n, int* group_count,

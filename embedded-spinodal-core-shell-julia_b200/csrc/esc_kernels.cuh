@@ -323,6 +323,8 @@ __global__ void __launch_bounds__(kBlock) k_final(const InstDev* __restrict__ in
   extern __shared__ __align__(16) unsigned char smraw[];
   cpx<SR>* sm = reinterpret_cast<cpx<SR>*>(smraw);
   const InstDev& I = insts[blockIdx.y];
+  // an instance stopped on a non-finite field keeps its input c (block-uniform)
+  if (*(volatile const int*)I.status) return;
   const int t = threadIdx.x % T, g = threadIdx.x / T;
   const int pair = blockIdx.x * G + g;
   const bool active = pair < H;

@@ -110,14 +110,15 @@ esc_status esc_batch_create(esc_batch **out, int count, const int *n, const doub
 /* Runs all instances for `steps` steps.  c[i] (n[i]^2, in/out) and history[i]
  * ((steps+1) x 6 each, entries may be NULL) are host arrays; bad_steps (count
  * entries, may be NULL) receives -1 or the step at which instance i became
- * non-finite.  Returns ESC_ENONFINITE if any instance did; the others still run
- * to the end and their outputs are valid. */
+ * non-finite.  Returns ESC_ENONFINITE if any instance did; such an instance's c
+ * is left unchanged and its history rows before that step are valid, while the
+ * others still run to the end and their outputs are valid. */
 esc_status esc_batch_run(esc_batch *b, double *const *c, int steps, double dt, double *const *history,
                          int64_t *bad_steps);
 
-/* Device-memory variant of esc_batch_run: c[i] are device pointers; history, if
- * not NULL, is ONE device array of count*(steps+1)*6 doubles, instance i at
- * offset i*(steps+1)*6. */
+/* Device-memory variant of esc_batch_run (same outputs, the same non-finite
+ * handling): c[i] are device pointers; history, if not NULL, is ONE device array
+ * of count*(steps+1)*6 doubles, instance i at offset i*(steps+1)*6. */
 esc_status esc_batch_run_device(esc_batch *b, double *const *c, int steps, double dt, double *history,
                                 int64_t *bad_steps);
 
