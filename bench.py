@@ -375,9 +375,12 @@ def main():
 
     def timed_device_run(precision, steps, warmup):
         b = esc.Batch(phis, params=ps, precision=precision)
-        stream = torch.cuda.current_stream()
+        # a dedicated (non-default) stream: the library forks its size groups from it and joins
+        # them back, and the CUDA events bracketing the K steps are recorded on it
+        stream = torch.cuda.Stream()
         b.set_stream(stream.cuda_stream)
         work = [c.clone() for c in dc0]
+        torch.cuda.synchronize()  # the clones ran on the default stream
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         # the sampler starts before the warm-up, so that its start-up pause does not
         # leave the GPU idle between the warm-up and the timed steps
