@@ -296,8 +296,9 @@ def batched_gradient_block(count=64, n=512, steps=1000):
     w = 2, sampled P, chi, kappa as in the ensemble), loss 1/2 |c_T - c_target|^2 + 1e-3 F[c_T]
     with c_target a forward run at (1.1 P, 0.9 chi), gradients w.r.t. (P, chi, kappa, M0)
     through `steps` steps for all particles in one esc_batch_adjoint call (mixed-precision
-    forward and recompute, FP64 adjoint).  Reports the gradient throughput and its cost
-    against a forward run of the same batch."""
+    forward and recompute, FP64 adjoint).  Reports the gradient throughput (and as a fraction
+    of the 64 B per pt-step roofline), its cost against a forward run of the same batch, and
+    the error of the gradients against the same call with an FP64 forward pass."""
     import esc
     ns, phis, c0s, ps = ensemble(count=count, seed_base=1000, sizes=(n,), rng_seed=7)
     pts = [esc.Parameters(A=p.A, B=p.B, chi=p.chi * 0.9, P=p.P * 1.1, ca=p.ca, cb=p.cb, cc=p.cc,
@@ -315,9 +316,20 @@ def batched_gradient_block(count=64, n=512, steps=1000):
         t0 = time.perf_counter()
         L, _, th = b.adjoint(c0s, targets, dt=DT, steps=steps, lambda_F=1e-3, with_field_gradients=False)
         t_adj = time.perf_counter() - t0
+    # the same gradients with an FP64 forward pass and recompute (the FP64 drop-in's arithmetic)
+    with esc.Batch(phis, params=ps, precision="fp64") as b64:
+        L64, _, th64 = b64.adjoint(c0s, targets, dt=DT, steps=steps, lambda_F=1e-3, with_field_gradients=False)
+    th, th64 = np.asarray(th), np.asarray(th64)
+    rel_th = np.max(np.abs(th - th64), axis=1) / np.max(np.abs(th64), axis=1)
+    rel_L = np.abs(np.asarray(L) - np.asarray(L64)) / np.abs(np.asarray(L64))
+    rate = count * n * n * steps / t_adj
     return {"particles": count, "n": n, "steps": steps, "gradient_call_s": t_adj, "forward_call_s": t_fwd,
-            "gradient_pt_steps_per_s": count * n * n * steps / t_adj,
+            "gradient_pt_steps_per_s": rate,
+            "gradient_step_frac_of_hbm_roofline": rate * B_ALG_PER_STEP / (read_peaks()[0] * 1e9),
             "gradient_call_over_forward_call": t_adj / t_fwd,
+            "vs_fp64_forward": {"dL_dtheta_rel_err_max": float(rel_th.max()),
+                                "dL_dtheta_rel_err_median": float(np.median(rel_th)),
+                                "L_rel_err_max": float(rel_L.max())},
             "dL_dtheta_particle0": [float(x) for x in th[0]], "L_particle0": float(L[0])}
 
 
