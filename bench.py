@@ -120,7 +120,7 @@ class ClockSampler:
     def summary(self):
         if not self.path or not os.path.exists(self.path):
             return None
-        sm, mx, reasons = [], [], set()
+        sm, mx, pw, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
@@ -131,6 +131,10 @@ class ClockSampler:
                 mx.append(float(parts[1]))
             except ValueError:
                 continue
+            try:
+                pw.append(float(parts[2]))
+            except ValueError:
+                pass
             for nm, v in zip(names, parts[3:7]):
                 if v.lower() == "active":
                     reasons.add(nm)
@@ -138,7 +142,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "power_w": statistics.median(pw) if pw else None, "samples": len(sm)}
 
 
 def cpu_oracle_rate(ns, phis, c0s, ps, steps, workers):
@@ -278,7 +282,8 @@ def single_grid_block(name, phi, c0, steps, peak_gbs):
 
 
 def large_grid_configs(peak_gbs):
-    """The two single-grid configurations: 1024^2 disc (R = 400, w = 2, c0 = 0.5 +
+    """The single-grid configurations: the default example of core_shell.jl (256^2, disc R = 70,
+    w = 4, interior noise, 1000 steps), the 1024^2 disc (R = 400, w = 2, c0 = 0.5 +
     U(-0.01, 0.01) over the whole field, seed 1) and the 4096^2 ellipse (semi-axes
     1600 along x and 1200 along y, w = 2, c0 = 0.5 + mean-free U(-0.01, 0.01)
     inside the particle, seed 5), 10,000 steps each, dt = 0.01."""
@@ -287,7 +292,10 @@ def large_grid_configs(peak_gbs):
     c02 = fields.whole_field_noise(1024, seed=1)
     phi5 = fields.particle_ellipse(4096, a=1600.0, b=1200.0, width=2.0)
     c05 = fields.interior_noise(phi5, 5)
-    return [single_grid_block("1024^2 disc R=400, 10000 steps", phi2, c02, 10000, peak_gbs),
+    phi0 = fields.particle_disc(256, radius=70.0, width=4.0)
+    c00 = fields.interior_noise(phi0, 5749)
+    return [single_grid_block("256^2 default example (disc R=70, w=4), 1000 steps", phi0, c00, 1000, peak_gbs),
+            single_grid_block("1024^2 disc R=400, 10000 steps", phi2, c02, 10000, peak_gbs),
             single_grid_block("4096^2 ellipse 1600x1200, 10000 steps", phi5, c05, 10000, peak_gbs)]
 
 
@@ -454,12 +462,13 @@ def main():
     fp64 = None
     max_err = None
     if not args.no_fp64:
-        bf, cf, ms64, _, _ = timed_device_run("fp64", args.steps, args.warmup)
+        bf, cf, ms64, clocks64, _ = timed_device_run("fp64", args.steps, args.warmup)
         ms64 = max_over_ranks(ms64)
         v64 = world * pts * args.steps / (ms64 / 1000.0)
         f_final = [w.cpu().numpy() for w in cf]
         max_err = max(float(np.max(np.abs(a - b))) for a, b in zip(bm_final, f_final))
         fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64 / args.steps, "speedup_mixed_over_fp64": value / v64,
+                "clocks": clocks64,
                 "kernel_families": [{k: g[k] for k in ("n", "rows", "cols")} for g in bf.describe()]}
         bf.close()
 
