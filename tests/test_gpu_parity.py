@@ -116,3 +116,14 @@ def test_mixed_large_against_fp64(n):
     assert rel(c32, c64) < 1e-5
     assert np.max(np.abs(h32[:, 1] - h32[0, 1])) < 1e-12
     assert np.max(np.abs(h32[:, 2] - h64[:, 2])) / np.max(np.abs(h64[:, 2])) < 1e-5
+
+
+@pytest.mark.parametrize("n,steps", [(64, 40), (96, 33), (192, 10)])
+def test_fp64_matches_c_oracle(n, steps):
+    """The second, independent CPU restatement (C with its own FFT) agrees as well."""
+    from oracle import c_oracle
+    c0, phi = case(n, seed=77)
+    c, h = esc.run_simulation(c0, phi, dt=0.01, steps=steps)
+    co, ho = c_oracle.run_simulation(c0, phi, dt=0.01, steps=steps)
+    assert rel(c, co) < RTOL_FP64
+    assert max(hist_rel(h, ho)) < RTOL_FP64
