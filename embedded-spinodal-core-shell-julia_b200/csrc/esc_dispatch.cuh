@@ -354,6 +354,11 @@ struct KS {
       if (alt_need > need) need = alt_need;
       const int wab = warp_partials();
       if (wab > need) need = wab;
+      // column A keeps one partial per warp after the row-A area (both column plans)
+      const int ca = 5 * tiles_pairs + ctiles * (CB / 32);
+      if (ca > need) need = ca;
+      const int caa = 5 * ((H + kBlock / AP::T - 1) / (kBlock / AP::T)) + alt_tiles_cols * (ColGeomF<AP, SR, WR>::B / 32);
+      if (caa > need) need = caa;
       k.part_len = need;
     }
     k.smem = smem();

@@ -125,6 +125,39 @@ __device__ __forceinline__ double reduce_partials(const double* p, int count, in
   return block_reduce<Op>(v, red);
 }
 
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Warp-level arrival: returns true (in every lane) in the warp that arrives
+// last among `total` arrivals; its earlier partial writes are then visible.
+__device__ __forceinline__ bool warp_arrive_last(unsigned* counter, unsigned total) {
+  unsigned last = 0;
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == total - 1) ? 1u : 0u;
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (last) __threadfence();
+  return last != 0;
+}
+
+// deterministic warp fold of `count` partials spaced `stride` apart.  The fold
+// runs in the last warp of an instance, and the last instance's fold ends the
+// launch, so its loads are unrolled to keep several in flight; each lane still
+// accumulates in increasing slot order.
+template <class Op>
+__device__ __forceinline__ double warp_fold(const double* p, int count, int stride, double init) {
+  double v = init;
+#pragma unroll 8
+  for (int i = (threadIdx.x & 31); i < count; i += 32) v = Op::ap(v, __ldcg(p + (size_t)i * stride));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = Op::ap(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 // ---- helpers -----------------------------------------------------------------
 template <typename R>
 __device__ __forceinline__ R wavenumber(int i, int n, double kunit) {
@@ -454,8 +487,6 @@ __global__ void __launch_bounds__(col_block<P, SR, WR>(), (col_min_blocks<P, SR,
                                                   int s_local) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeomF<P, SR, WR>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double red[32];
-  __shared__ int lastflag;
   const InstDev& I = insts[blockIdx.y];
   const int status = *(volatile const int*)I.status;  // read after the column loads are issued
   const int w = threadIdx.x % W, t = threadIdx.x / W;
@@ -574,13 +605,14 @@ __global__ void __launch_bounds__(col_block<P, SR, WR>(), (col_min_blocks<P, SR,
       Gp[(size_t)(t + T * m) * H + kx] = o;
     }
   }
-  const double r = block_reduce<OpSum>(gsum, red);
-  const int tiles = gridDim.x;
+  // per-warp partials and a per-warp arrival: no block-wide barrier at the end
+  const double r = warp_sum(gsum);
+  const int nw = (int)(blockDim.x >> 5), slots = (int)gridDim.x * nw;
   double* part = I.part + (size_t)5 * ((H + RowGeom<P>::G - 1) / RowGeom<P>::G);
-  if (threadIdx.x == 0) part[blockIdx.x] = r;
-  if (!arrive_last(&I.cnt[1], tiles, &lastflag)) return;
-  const double gr = reduce_partials<OpSum>(part, tiles, 1, 0.0, red);
-  if (threadIdx.x == 0) {
+  if ((threadIdx.x & 31) == 0) part[blockIdx.x * nw + (threadIdx.x >> 5)] = r;
+  if (!warp_arrive_last(&I.cnt[1], (unsigned)slots)) return;
+  const double gr = warp_fold<OpSum>(part, slots, 1, 0.0);
+  if ((threadIdx.x & 31) == 0) {
     const int s = step_index(base, s_local);
     if (I.hist) {
       const double e = (I.scal[0] + kappa * gr / ((double)N * N)) * I.dx * I.dx;

@@ -82,11 +82,6 @@ struct WarpRowGeom {
   }
 };
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 __device__ __forceinline__ double warp_min(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -98,32 +93,7 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// Warp-level arrival: returns true (in every lane) in the warp that arrives
-// last among `total` arrivals; its earlier partial writes are then visible.
-__device__ __forceinline__ bool warp_arrive_last(unsigned* counter, unsigned total) {
-  unsigned last = 0;
-  if ((threadIdx.x & 31) == 0) {
-    __threadfence();
-    last = (atomicAdd(counter, 1u) == total - 1) ? 1u : 0u;
-  }
-  last = __shfl_sync(0xffffffffu, last, 0);
-  if (last) __threadfence();
-  return last != 0;
-}
 
-// deterministic warp fold of `count` partials spaced `stride` apart.  The fold
-// runs in the last warp of an instance, and the last instance's fold ends the
-// launch, so its loads are unrolled to keep several in flight; each lane still
-// accumulates in increasing slot order.
-template <class Op>
-__device__ __forceinline__ double warp_fold(const double* p, int count, int stride, double init) {
-  double v = init;
-#pragma unroll 8
-  for (int i = (threadIdx.x & 31); i < count; i += 32) v = Op::ap(v, __ldcg(p + (size_t)i * stride));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = Op::ap(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
 
 // The five row-A folds (sum c, min c, max c, sum f, non-finite count) of slots
 // holding five consecutive doubles, in one pass: one slot's five loads are
