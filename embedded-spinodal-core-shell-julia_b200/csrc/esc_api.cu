@@ -389,6 +389,9 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
       d.tw_w = g.tw_w;
       d.cio = g.cio + s * nn;
     }
+    // valid descriptors from creation on (no history, dt = 0 until a run sets them), so that
+    // no kernel can ever read an unwritten descriptor
+    CK(cudaMemcpy(g.d_inst, g.h_inst.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice));
     CK(cudaMemset(g.cnt, 0, cnt * 4 * sizeof(unsigned)));
     CK(cudaMemset(g.status, 0, cnt * sizeof(int)));
     if (g.ks->warp_rows) {
