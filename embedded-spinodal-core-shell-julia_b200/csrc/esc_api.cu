@@ -462,7 +462,8 @@ void phase_col_b(Group& g, cudaStream_t st) {
 // B, on a smooth synthetic state, and keeps the fastest.  Decisions are cached
 // per process by (n, precision, instances) and, when ESC_TUNE_CACHE names a
 // file, read from / appended to it so that later processes reuse them.
-// ESC_TUNE=0 skips timing and takes the warp rows and legacy columns.
+// ESC_TUNE=0 skips timing and takes the warp rows and legacy columns; it and a
+// family forced with ESC_ROWS / ESC_COLS bypass the cached decisions.
 struct TuneKey {
   int n, prec, count;
   bool operator<(const TuneKey& o) const {
@@ -519,7 +520,9 @@ esc_status autotune(Engine& E) {
     const bool can_pipe_rows = g.pipe_rows, can_warp = g.warp_rows, can_pipe_cols = g.pipe_cols;
     const TuneKey key{g.n, E.prec, (int)g.members.size()};
     auto hit = tune_cache().find(key);
-    if (hit != tune_cache().end()) {
+    // a family forced by ESC_ROWS / ESC_COLS, or ESC_TUNE=0, takes precedence over cached decisions
+    const bool use_cache = tuning_enabled() && row_family_override() < 0 && col_family_override() < 0;
+    if (use_cache && hit != tune_cache().end()) {
       int r = hit->second.first, k = hit->second.second;
       if ((r == 2 && !can_warp) || (r == 1 && !can_pipe_rows)) r = 0;
       apply_rows(g, r);
@@ -529,10 +532,9 @@ esc_status autotune(Engine& E) {
     if (!timing) {
       if (row_family_override() < 0) apply_rows(g, can_warp ? 2 : (can_pipe_rows ? 1 : 0));
       else g.row_family = g.warp_rows ? 2 : (g.pipe_rows ? 1 : 0);
-      g.col_family = g.pipe_cols ? 1 : 0;
-      if (row_family_override() < 0 && pipeline_enabled()) apply_cols(g, 0);
+      // columns: the block kernels unless ESC_COLS asks for a family this size can run
       const int cfo = col_family_override();
-      if ((cfo == 1 && can_pipe_cols) || (cfo == 2 && g.ks->E_alt != g.ks->E)) apply_cols(g, cfo);
+      apply_cols(g, ((cfo == 1 && can_pipe_cols) || (cfo == 2 && g.ks->E_alt != g.ks->E)) ? cfo : 0);
       continue;
     }
     any = true;
@@ -614,9 +616,11 @@ esc_status autotune(Engine& E) {
     g.pipe_rows = can_pipe_rows;
     g.warp_rows = can_warp;
     apply_rows(g, best_rf);
-    const TuneKey key{g.n, E.prec, (int)g.members.size()};
-    tune_cache()[key] = {best_rf, best_cf};
-    save_tune(key, best_rf, best_cf);
+    if (col_family_override() < 0) {  // a forced column family is not a decision to keep
+      const TuneKey key{g.n, E.prec, (int)g.members.size()};
+      tune_cache()[key] = {best_rf, best_cf};
+      save_tune(key, best_rf, best_cf);
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
