@@ -82,6 +82,15 @@ struct WarpRowGeom {
   }
 };
 
+// Resident blocks per SM row A is compiled for: E8 in 64-thread groups runs
+// 16 (mixed) or 14 (FP64) two-warp blocks, a few bytes of spills against 12 at
+// 80 registers (row A at n = 512: 4 % and 2 % faster); other plans keep their
+// group geometry's figure.
+template <class P, typename SR, typename WR>
+constexpr int row_a_minb() {
+  return (P::T == 64 && P::E <= 8) ? (kSplitMixed<SR, WR> ? 16 : 14) : WarpRowGeom<P>::MINB;
+}
+
 __device__ __forceinline__ double warp_min(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -144,7 +153,7 @@ __device__ __forceinline__ bool warp_status_running(int s) { return __shfl_sync(
 
 // =====================================================================================
 template <class P, typename SR, typename WR>
-__global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, WarpRowGeom<P>::MINB) k_row_a_w(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(WarpRowGeom<P>::BLOCK, (row_a_minb<P, SR, WR>())) k_row_a_w(const InstDev* __restrict__ insts,
                                                        const int* __restrict__ base, int s_local) {
   using WG = WarpRowGeom<P>;
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, NW = WG::NW, G = WG::G;
