@@ -61,7 +61,9 @@ struct WarpRowGeom {
                 "groups inside one warp, or a block of 64, 128 or 256 threads");
   static constexpr int BLOCK = kInWarp ? kWarpBlock : T;  // threads per block
   // blocks per SM compiled for: 128 registers per thread for T >= 128
-  static constexpr int MINB = kInWarp ? kWarpBlocksPerSM : (T == 64 ? (P::E <= 8 ? 12 : 8) : 512 / T);
+  // (whole-warp groups of at most 12 elements fit 20 blocks, 96 registers, without spills: n = 384)
+  static constexpr int MINB =
+      kInWarp ? ((T == 32 && P::E <= 12) ? 20 : kWarpBlocksPerSM) : (T == 64 ? (P::E <= 8 ? 12 : 8) : 512 / T);
   static constexpr int GPW = kInWarp ? 32 / T : 1;        // groups per warp
   static constexpr int NW = BLOCK / 32;                   // warps per block
   static constexpr int G = kInWarp ? GPW * NW : 1;        // groups per block
