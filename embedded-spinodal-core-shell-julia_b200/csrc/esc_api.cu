@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -88,6 +89,16 @@ struct Group {
   int row_family = -1, col_family = -1;
   float row_ms[3] = {-1, -1, -1}, col_ms[3] = {-1, -1, -1};
 };
+
+// Creating a context touches state shared by every context of the process: the
+// tuner's decision cache and its file, the occupancy table of the persistent
+// kernels and the tensor-map encoder lookup.  Creations are therefore
+// serialised under this lock; running, profiling and destroying contexts take
+// no lock.
+std::mutex& creation_mutex() {
+  static std::mutex m;
+  return m;
+}
 
 // cuTensorMapEncodeTiled from the driver, looked up once
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -1220,9 +1231,13 @@ esc_status esc_create(esc_ctx** out, int n, double dx, const double* phi, const 
     return ESC_ENOMEM;
   }
   const double* phis[1] = {phi};
-  esc_status s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
-  if (s == ESC_OK) s = autotune(c->e);
-  if (s == ESC_OK) s = ensure_graph(c->e);
+  esc_status s;
+  {
+    std::lock_guard<std::mutex> lock(creation_mutex());
+    s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
+    if (s == ESC_OK) s = autotune(c->e);
+    if (s == ESC_OK) s = ensure_graph(c->e);
+  }
   if (s != ESC_OK) {
     tl_err = c->e.err;
     c->e.release();
@@ -1287,9 +1302,13 @@ esc_status esc_batch_create(esc_batch** out, int count, const int* n, const doub
     tl_err = "host allocation failed";
     return ESC_ENOMEM;
   }
-  esc_status s = engine_create(b->e, count, n, dx, phi, p, (int)prec);
-  if (s == ESC_OK) s = autotune(b->e);
-  if (s == ESC_OK) s = ensure_graph(b->e);
+  esc_status s;
+  {
+    std::lock_guard<std::mutex> lock(creation_mutex());
+    s = engine_create(b->e, count, n, dx, phi, p, (int)prec);
+    if (s == ESC_OK) s = autotune(b->e);
+    if (s == ESC_OK) s = ensure_graph(b->e);
+  }
   if (s != ESC_OK) {
     tl_err = b->e.err;
     b->e.release();

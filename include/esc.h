@@ -19,6 +19,8 @@
  *   - Functions return esc_status and never exit, abort or trap.  The message of
  *     the last failure is available from esc_last_error / esc_batch_last_error.
  *   - One context per host thread at a time; calls on a context are not re-entrant.
+ *     Contexts on different threads run concurrently; their creations
+ *     (esc_create, esc_batch_create) are serialised inside the library.
  */
 #ifndef ESC_H
 #define ESC_H

@@ -102,3 +102,34 @@ def test_no_gpu_fails_loudly_not_silently():
     with pytest.raises(esc.EscError) as ei:
         esc.Context(np.zeros((64, 64)))
     assert ei.value.status in (esc.ESC_ECUDA, esc.ESC_ENOMEM)
+
+
+def test_concurrent_creations_fail_independently():
+    """Creations from many host threads at once (they are serialised inside the
+    library): every call returns, the lock is released on each error path, and
+    each thread reads its own message from esc_last_error(NULL).  All of them fail
+    argument validation, so no CUDA call is made."""
+    import threading
+    lib = esc.load_library()
+    cp = esc._CParams.of(esc.Parameters())
+    results = {}
+
+    def attempt(i):
+        h = ctypes.c_void_p()
+        n = 100 + 2 * i                      # no kernels for these sizes
+        phi = np.zeros((n, n))
+        for _ in range(50):
+            st = lib.esc_create(ctypes.byref(h), n, 1.0, phi.ctypes.data_as(esc._dp), ctypes.byref(cp), 0)
+            msg = lib.esc_last_error(None)
+            if st != esc.ESC_EINVAL or h.value or f"unsupported grid size {n}".encode() not in msg:
+                results[i] = (st, h.value, msg)
+                return
+        results[i] = "ok"
+
+    threads = [threading.Thread(target=attempt, args=(i,)) for i in range(8)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=60)
+    assert not any(t.is_alive() for t in threads)
+    assert results == {i: "ok" for i in range(8)}
