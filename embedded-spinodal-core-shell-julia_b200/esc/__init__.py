@@ -119,6 +119,7 @@ _SIGNATURES = [
                                            _vp, _vp]),
     ("esc_noise_device", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
                                         _vp, _vp]),
+    ("esc_julia_rand", ctypes.c_int, [ctypes.c_uint64, _dp, ctypes.c_int64]),
     ("esc_batch_last_error", ctypes.c_char_p, [_vp]),
     ("esc_batch_destroy", None, [_vp]),
 ]

@@ -2,17 +2,31 @@
 
 These build the inputs of a run: the tanh disc and initial composition of
 ``initial_fields`` (reference core_shell.jl:27-37), an elliptical particle, and
-whole-field noise for ensembles.  Noise comes from NumPy's PCG64 with the given
-seed (Julia's MersenneTwister stream is not reproducible outside Julia); the
-distribution -- uniform in [-amplitude, amplitude), mean removed over the
-particle interior -- is the reference's.  Arrays are C-ordered ``a[y, x]``
-(the bytes of the column-major Julia matrix).
+whole-field noise for ensembles.  Noise is the reference's own stream:
+``rand(MersenneTwister(seed), n, n)`` (core_shell.jl:32), reproduced bit for bit
+by the library's host function ``esc_julia_rand`` (Julia 1.12's seed hashing and
+dSFMT-19937), so ``initial_fields(n; radius, width, seed)`` returns exactly the
+reference's inputs.  Arrays are C-ordered ``a[y, x]`` (the bytes of the
+column-major Julia matrix).
 """
 from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["particle_disc", "particle_ellipse", "interior_noise", "whole_field_noise", "initial_fields"]
+__all__ = ["particle_disc", "particle_ellipse", "julia_rand", "interior_noise", "whole_field_noise",
+           "initial_fields"]
+
+
+def julia_rand(seed: int, n: int, m: int | None = None) -> np.ndarray:
+    """``rand(MersenneTwister(seed), n, m)`` as a C-ordered array ``a[j, i]`` (esc_julia_rand)."""
+    from . import _ptr, _raise, load_library
+    m = n if m is None else m
+    out = np.empty((m, n), dtype=np.float64)
+    lib = load_library()
+    st = lib.esc_julia_rand(int(seed) & 0xFFFFFFFFFFFFFFFF, _ptr(out), out.size)
+    if st != 0:
+        _raise(st, "esc_julia_rand: bad arguments")
+    return out
 
 
 def _centred(n: int, spacing: float) -> np.ndarray:
@@ -35,10 +49,10 @@ def particle_ellipse(n: int, a: float, b: float, width: float, spacing: float = 
 
 
 def interior_noise(phi: np.ndarray, seed: int, amplitude: float = 0.01, mean: float = 0.5) -> np.ndarray:
-    """c = mean everywhere plus, inside (phi >= 0.5), uniform noise with its
-    interior mean removed (core_shell.jl:31-35)."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    noise = amplitude * (2.0 * rng.random(phi.shape) - 1.0)
+    """c = mean everywhere plus, inside (phi >= 0.5), uniform noise
+    amplitude (2 rand(MersenneTwister(seed), n, n) - 1) with its interior mean
+    removed (core_shell.jl:31-35)."""
+    noise = amplitude * (2.0 * julia_rand(seed, phi.shape[1], phi.shape[0]) - 1.0)
     inside = phi >= 0.5
     c = np.full(phi.shape, mean, dtype=np.float64)
     if inside.any():
@@ -48,9 +62,8 @@ def interior_noise(phi: np.ndarray, seed: int, amplitude: float = 0.01, mean: fl
 
 
 def whole_field_noise(n: int, seed: int, mean: float = 0.5, amplitude: float = 0.01) -> np.ndarray:
-    """c0 = mean + U(-amplitude, amplitude) on every point."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    return mean + amplitude * (2.0 * rng.random((n, n)) - 1.0)
+    """c0 = mean + amplitude (2 rand(MersenneTwister(seed), n, n) - 1) on every point."""
+    return mean + amplitude * (2.0 * julia_rand(seed, n) - 1.0)
 
 
 def initial_fields(n: int, spacing: float = 1.0, radius: float = 70.0, width: float = 4.0, seed: int = 5749):

@@ -189,6 +189,15 @@ esc_status esc_particle_device(int shape, int n, double dx, const double *params
 esc_status esc_noise_device(int n, const double *phi, double mean, double amplitude, uint64_t seed, double *c,
                             void *stream);
 
+/* Fills out[0..count) with the first `count` values of Julia's
+ * rand(MersenneTwister(seed), count): the stream the reference's initial_fields
+ * draws its noise from (core_shell.jl:32, rand(MersenneTwister(seed), n, n) in
+ * the memory order of the n x n matrix).  The seed is hashed with SHA2-256 into
+ * the key of dSFMT-19937, as Julia 1.12's Random library does, and the values lie
+ * in [0, 1).  Host code only (no GPU); replaces nothing on the time loop, it
+ * reproduces the reference's inputs. */
+esc_status esc_julia_rand(uint64_t seed, double *out, int64_t count);
+
 /* Allocation-free single-particle run.  No counterpart in the reference: it
  * exists for callers that may not call cudaMalloc themselves or through this
  * library (device memory owned by another allocator or a fixed budget, or a

@@ -1,7 +1,8 @@
 """Generates the golden fixtures in this directory from the CPU oracle.
 
 Run from the repository root:  python tests/golden/make_golden.py
-Each fixture holds the inputs (c0, phi, parameters, dt, steps) and the oracle's
+Each fixture holds the inputs (c0, phi, parameters, dt, steps; c0 from the
+reference's own noise stream, initial_fields) and the oracle's
 outputs (final c, history) of a short run of run_simulation
 (core_shell.jl:84-103).  The GPU parity tests compare the CUDA library with
 these files; the CPU tests re-run the oracle and compare it with them, which
