@@ -550,8 +550,16 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    mix_acc = (accuracy or {}).get("mixed_vs_fp64") or {}
+    targets = {  # the north-star targets next to what this run measured
+        "step_frac_of_hbm_roofline": roofline["step_frac"], "step_frac_target": 0.60,
+        "mixed_over_fp64": (value / fp64["value"]) if fp64 else None, "mixed_over_fp64_target": 5.0,
+        "frac_instances_within_1e-5": mix_acc.get("frac_instances_le_1e-5"), "within_1e-5_target": 1.0,
+    }
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "unit": UNIT,
+        "fp64_dropin_value": fp64["value"] if fp64 else None, "targets": targets,
+        "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 state / f32 flux transforms",
         "data": "synthetic",

@@ -137,6 +137,14 @@ bool pipeline_enabled() {
   return !(v && v[0] == '0');
 }
 
+// ESC_PIPE_DROP_COPY = 1 (read at creation; a test knob): the TMA pipeline kernels
+// withhold their first tile copy, so that the bounded wait for it runs out and the
+// run reports ESC_ETIMEOUT.  Nothing is left in flight: no copy was issued for it.
+bool drop_copy_knob() {
+  const char* v = getenv("ESC_PIPE_DROP_COPY");
+  return v && v[0] == '1';
+}
+
 // ESC_ROWS = warp | pipe | legacy forces one row-kernel family (measurement aid)
 int row_family_override() {
   const char* v = getenv("ESC_ROWS");
@@ -399,6 +407,7 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
       d.tw_s = g.tw_s;
       d.tw_w = g.tw_w;
       d.cio = g.cio + s * nn;
+      d.drop_first_copy = drop_copy_knob() ? 1 : 0;
     }
     // valid descriptors from creation on (no history, dt = 0 until a run sets them), so that
     // no kernel can ever read an unwritten descriptor

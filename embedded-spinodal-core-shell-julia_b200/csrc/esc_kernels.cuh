@@ -63,6 +63,8 @@ struct InstDev {
   const void* tw_s;   // twiddles e^{-2 pi i j/n} in SR
   const void* tw_w;   // same in WR
   double* cio;        // real FP64 field for init/final (n*n)
+  int drop_first_copy; // test knob (ESC_PIPE_DROP_COPY): the TMA pipeline kernels skip their
+                       // first copy and their bounded wait for it runs out (ESC_ETIMEOUT)
 };
 
 // ---- reductions --------------------------------------------------------------

@@ -19,8 +19,15 @@
 //   * calls that overlap on the GPU (different host threads or streams at the
 //     same time) race on the array and must be serialised by the caller;
 //   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture begins.
+//     cudaGetSymbolAddress (once per device, with that device current);
+//   * no call may run inside a stream capture: each call copies its small
+//     descriptor from host memory and waits for its stream, neither of which a
+//     capture allows, so a call on a capturing stream returns ESC_EINVAL
+//     without touching the stream;
+//   * the pass-major twiddle tables of a grid size are process-wide __device__
+//     arrays; the first call for a size on a device fills them, later calls
+//     reuse them.  Creating a context of the same size refills them with
+//     identical values, so a kernel reading them meanwhile sees the same bits.
 // The array is part of the library image: every GPU that loads libesc.so
 // holds it (about 2.1 MiB) until the process exits.
 #include <cuda_runtime.h>
@@ -83,6 +90,7 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
+bool g_tables_filled[kMaxDevices][kNoAllocMaxN + 1] = {};  // pass-major tables of size n filled on a device
 
 esc_status fail(esc_status s, const char* what, cudaError_t e = cudaSuccess) {
   char msg[256];
@@ -123,8 +131,14 @@ extern "C" esc_status esc_run_noalloc(int n, double dx, const double* phi, const
     }
     base = g_scratch_ptr[dev];
   }
-  if ((e = ks->prepare()) != cudaSuccess) return fail(ESC_ECUDA, "kernel attributes", e);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(st, &cs)) != cudaSuccess) return fail(ESC_ECUDA, "cudaStreamIsCapturing", e);
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(ESC_EINVAL, "esc_run_noalloc: cannot be called while the stream is being captured");
+  }
+  if ((e = ks->prepare()) != cudaSuccess) return fail(ESC_ECUDA, "kernel attributes", e);
 
   // twiddles e^{-2 pi i j/n} in long double, staged on the host stack
   double tw[2 * kNoAllocMaxN];
@@ -163,7 +177,15 @@ extern "C" esc_status esc_run_noalloc(int n, double dx, const double* phi, const
     if (e_ != cudaSuccess) return fail(ESC_ECUDA, #call, e_); \
   } while (0)
   NA_CK(cudaMemcpyAsync(base + kOffTw, tw, (size_t)n * 16, cudaMemcpyHostToDevice, st));
-  ks->fill_tables(base + kOffTw, base + kOffTw, st);  // the pass-major tables are fixed __device__ arrays too
+  {
+    // the pass-major tables are fixed __device__ arrays too: filled by the first call of this size
+    std::lock_guard<std::mutex> lock(g_setup_mu);
+    if (!g_tables_filled[dev][n]) {
+      ks->fill_tables(base + kOffTw, base + kOffTw, st);
+      NA_CK(cudaGetLastError());
+      g_tables_filled[dev][n] = true;
+    }
+  }
   NA_CK(cudaMemcpyAsync(base + kOffInst, &d, sizeof d, cudaMemcpyHostToDevice, st));
   // state that must start at zero: counters, status, bad step (-1), step counter
   NA_CK(cudaMemsetAsync(base + kOffCnt, 0, 256, st));
@@ -186,6 +208,9 @@ extern "C" esc_status esc_run_noalloc(int n, double dx, const double* phi, const
   NA_CK(cudaMemcpyAsync(&status, base + kOffStatus, sizeof status, cudaMemcpyDeviceToHost, st));
   NA_CK(cudaMemcpyAsync(&bad, base + kOffBad, sizeof bad, cudaMemcpyDeviceToHost, st));
   NA_CK(cudaStreamSynchronize(st));
+  if (status == esc::kStatusLayout)
+    return fail(ESC_ECUDA, "esc_run_noalloc: internal error: a shared-memory stage was misaligned");
+  if (status == esc::kStatusTimeout) return fail(ESC_ETIMEOUT, "esc_run_noalloc: a bounded device-side wait gave up");
   if (status) {
     if (bad_step) *bad_step = bad;
     char msg[96];

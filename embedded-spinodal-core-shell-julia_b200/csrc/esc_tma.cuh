@@ -44,11 +44,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: gives up after `limit` polls (each poll may suspend briefly in
-// hardware) and returns false, so a copy that never lands cannot hang the GPU.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit = 1u << 24) {
-  for (uint32_t i = 0; i < limit; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// A legitimate wait for a tile copy lasts microseconds; one second means the
+// copy is not coming.  The drain after a failed wait uses a shorter bound.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+constexpr uint64_t kDrainLimitNs = 200000000ull;
+
+// Bounded wait: polls until the phase completes, or until `limit_ns` of global
+// time have passed (or, as a last resort, 2^30 polls), and then returns false,
+// so a copy that never lands cannot hang the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t round = 0; round < (1u << 25); ++round) {
+#pragma unroll 1
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
+  }
   return false;
 }
 

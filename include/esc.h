@@ -208,10 +208,14 @@ esc_status esc_julia_rand(uint64_t seed, double *out, int64_t count);
  * library (about 2.1 MiB per GPU, held until exit), so n is limited to 256:
  * larger n returns ESC_EINVAL.  All calls share that array: calls that overlap on
  * the GPU race and must be serialised by the caller.  The first call on a device
- * looks up the array's address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Work is queued on `stream` (a cudaStream_t, NULL = default
- * stream) and the call returns when it has finished.  Failures are described by
- * esc_last_error(NULL). */
+ * looks up the array's address (cudaGetSymbolAddress).  No call can run inside a
+ * stream capture (each call copies a host descriptor and waits for its stream);
+ * a call on a capturing stream returns ESC_EINVAL.  The first call of a grid size
+ * on a device fills that size's process-wide twiddle tables; creating a context of
+ * the same size rewrites them with identical values, which is harmless to kernels
+ * reading them at that moment.  Work is queued on `stream` (a cudaStream_t, NULL =
+ * default stream) and the call returns when it has finished.  Failures are
+ * described by esc_last_error(NULL). */
 esc_status esc_run_noalloc(int n, double dx, const double *phi, const esc_params *p, double *c, int steps,
                            double dt, double *history, int64_t *bad_step, void *stream);
 void esc_batch_destroy(esc_batch *b);

