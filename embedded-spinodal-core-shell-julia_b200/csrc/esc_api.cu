@@ -29,19 +29,34 @@
 #define ESC_DECL(n) const esc::KernelSet* esc_kernels_##n(int prec);
 ESC_SIZES(ESC_DECL)
 #undef ESC_DECL
+// runtime-size kernel sets (esc_generic.cu)
+const esc::KernelSet* esc_generic_kernels(int n, int prec);
+int esc_generic_supported(int n);
 
 namespace {
 
+// ESC_GENERIC = 1 (a validation knob): use the runtime-size kernels even where a
+// tuned kernel set exists, so that tests can compare them with the oracle at any n.
+bool force_generic() {
+  const char* v = getenv("ESC_GENERIC");
+  return v && v[0] == '1';
+}
+
+// The tuned, compile-time kernel set of n, else the runtime-size set (any n the
+// reference accepts within esc_generic_supported), else null.
 const esc::KernelSet* find_kernels(int n, int prec) {
-  switch (n) {
+  if (!force_generic()) {
+    switch (n) {
 #define ESC_CASE(nn) \
   case nn:           \
     return esc_kernels_##nn(prec);
-    ESC_SIZES(ESC_CASE)
+      ESC_SIZES(ESC_CASE)
 #undef ESC_CASE
-    default:
-      return nullptr;
+      default:
+        break;
+    }
   }
+  return esc_generic_kernels(n, prec);
 }
 
 thread_local std::string tl_err;
@@ -307,7 +322,7 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
   for (int i = 0; i < count; ++i) {
     if (!esc_supported_size(n[i]))
       return E.fail(ESC_EINVAL, "unsupported grid size " + std::to_string(n[i]) +
-                                    " (need even n = 2^a 3^b, 8 <= n <= 4096)");
+                                    " (need 2 <= n <= 4096 with every prime factor <= 127, or n <= 512)");
     if (!(dx[i] > 0.0) || !std::isfinite(dx[i])) return E.fail(ESC_EINVAL, "spacing must be positive and finite");
     if (!phi[i]) return E.fail(ESC_EINVAL, "null particle field");
     if (!finite_params(p[i])) return E.fail(ESC_EINVAL, "non-finite model parameter");
@@ -345,9 +360,10 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
     const size_t cnt = g.members.size();
     const size_t nn = (size_t)g.n * g.n;
     const size_t sr = g.ks->sr_bytes, wr = g.ks->wr_bytes;
-    TRY(E.alloc(&g.S, cnt * nn * sr, "state buffer"));
-    TRY(E.alloc(&g.F, cnt * nn * wr, "f' buffer"));
-    TRY(E.alloc(&g.G, cnt * nn * 2 * wr, "flux buffer"));
+    const size_t fe = g.ks->cplx_per_field;  // complex elements per field and instance
+    TRY(E.alloc(&g.S, cnt * fe * 2 * sr, "state buffer"));
+    TRY(E.alloc(&g.F, cnt * fe * 2 * wr, "f' buffer"));
+    TRY(E.alloc(&g.G, cnt * fe * 4 * wr, "flux buffer"));
     TRY(E.alloc(&g.phi, cnt * nn * wr, "particle buffer"));
     TRY(E.alloc(&g.tw_s, (size_t)g.n * 2 * sr, "twiddles"));
     TRY(E.alloc(&g.tw_w, (size_t)g.n * 2 * wr, "twiddles"));
@@ -395,9 +411,9 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
       d.n = g.n;
       d.dx = E.dx[i];
       d.p = E.p[i];
-      d.S = static_cast<char*>(g.S) + s * nn * sr;
-      d.F = static_cast<char*>(g.F) + s * nn * wr;
-      d.G = static_cast<char*>(g.G) + s * nn * 2 * wr;
+      d.S = static_cast<char*>(g.S) + s * fe * 2 * sr;
+      d.F = static_cast<char*>(g.F) + s * fe * 2 * wr;
+      d.G = static_cast<char*>(g.G) + s * fe * 4 * wr;
       d.phi = static_cast<char*>(g.phi) + s * nn * wr;
       d.part = g.part + s * (size_t)g.ks->part_len;
       d.cnt = g.cnt + s * 4;

@@ -15,6 +15,8 @@ struct KernelSet {
   int part_len;  // partial-sum doubles per instance
   size_t smem;   // dynamic shared memory per block
   size_t sr_bytes, wr_bytes;  // sizeof(real) of the state and work types
+  size_t cplx_per_field;      // complex elements of S (and of F; G holds twice as many) per instance
+  bool generic;               // runtime-size kernels (esc_generic.cu): no tuned families, no adjoint
   cudaError_t (*prepare)();
   cudaError_t (*prepare_pipe)();
   // fills the pass-major twiddle tables of every plan the set uses from the
@@ -364,6 +366,8 @@ struct KS {
     k.smem = smem();
     k.sr_bytes = sizeof(SR);
     k.wr_bytes = sizeof(WR);
+    k.cplx_per_field = (size_t)N * N / 2;  // H x n, the (DC, Nyquist) pair packed in slot 0
+    k.generic = false;
     k.prepare = &prepare;
     k.fill_tables = &fill_tables;
     k.init = &init;

@@ -110,7 +110,7 @@ extern "C" esc_status esc_run_noalloc(int n, double dx, const double* phi, const
   if (n > kNoAllocMaxN)
     return fail(ESC_EINVAL, "esc_run_noalloc: grid size above the fixed scratch limit of 256");
   const esc::KernelSet* ks = lookup(n);
-  if (!ks) return fail(ESC_EINVAL, "esc_run_noalloc: unsupported grid size (need even n = 2^a 3^b, 8 <= n <= 256)");
+  if (!ks) return fail(ESC_EINVAL, "esc_run_noalloc: unsupported grid size (needs a tuned size: 8, 12, 16, 24, 32, 48, 64, 96, 128, 192 or 256)");
   if (!phi || !c || !p) return fail(ESC_EINVAL, "esc_run_noalloc: null argument");
   if (!(dx > 0.0) || !std::isfinite(dx) || !std::isfinite(dt) || steps < 0)
     return fail(ESC_EINVAL, "esc_run_noalloc: bad spacing, dt or step count");

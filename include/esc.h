@@ -15,7 +15,12 @@
  *   - history is (steps+1) x 6 Float64, column-major like Julia's
  *     zeros(steps+1, 6): row s (0-based) at history[s + col*(steps+1)].
  *   - All pointers are host memory unless a function name says `_device`.
- *   - Supported grid sizes: even n = 2^a 3^b with 8 <= n <= 4096 (esc_supported_size).
+ *   - Supported grid sizes (esc_supported_size): any n with 2 <= n <= 4096 whose prime
+ *     factors are all <= 127, and any n <= 512, odd n included (the reference's make_grid
+ *     and FFTW take any n, core_shell.jl:17-25).  Tuned kernel sets serve
+ *     n = 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048,
+ *     3072, 4096; every other size runs on runtime-size kernels with the same results.
+ *     esc_adjoint, esc_batch_adjoint and esc_run_noalloc need a tuned size.
  *   - Functions return esc_status and never exit, abort or trap.  The message of
  *     the last failure is available from esc_last_error / esc_batch_last_error.
  *   - One context per host thread at a time; calls on a context are not re-entrant.

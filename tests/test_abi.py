@@ -49,11 +49,14 @@ def test_default_params_match_reference():
 
 
 def test_supported_sizes():
+    # tuned kernel sets
     ok = [8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096]
+    # runtime-size kernels: any n in [2, 4096] with prime factors <= 127, or any n <= 512 (odd, prime, radix 5, 7)
+    ok += [2, 3, 4, 6, 10, 15, 65, 97, 100, 101, 130, 160, 255, 320, 509, 1000, 2187, 4095]
     for n in ok:
-        assert esc.supported_size(n)
-    for n in (0, 4, 6, 10, 100, 130, 4097, 8192, 65, 255, -8):
-        assert not esc.supported_size(n)
+        assert esc.supported_size(n), n
+    for n in (0, 1, -8, 4097, 8192, 521, 1009, 4093, 2 * 257 * 3):
+        assert not esc.supported_size(n), n
     assert b"sm_100a" in esc.load_library().esc_version()
 
 
@@ -61,10 +64,10 @@ def test_invalid_arguments_rejected_before_cuda():
     lib = esc.load_library()
     cp = esc._CParams.of(esc.Parameters())
     h = ctypes.c_void_p()
-    phi = np.zeros((100, 100))
-    st = lib.esc_create(ctypes.byref(h), 100, 1.0, phi.ctypes.data_as(esc._dp), ctypes.byref(cp), 0)
+    phi = np.zeros((1009, 1009))
+    st = lib.esc_create(ctypes.byref(h), 1009, 1.0, phi.ctypes.data_as(esc._dp), ctypes.byref(cp), 0)
     assert st == esc.ESC_EINVAL and not h.value
-    assert b"unsupported grid size 100" in lib.esc_last_error(None)
+    assert b"unsupported grid size 1009" in lib.esc_last_error(None)
     st = lib.esc_create(ctypes.byref(h), 64, 1.0, None, ctypes.byref(cp), 0)
     assert st == esc.ESC_EINVAL
     phi = np.zeros((64, 64))
@@ -116,7 +119,7 @@ def test_concurrent_creations_fail_independently():
 
     def attempt(i):
         h = ctypes.c_void_p()
-        n = 100 + 2 * i                      # no kernels for these sizes
+        n = (521, 523, 541, 547, 557, 563, 569, 571)[i]   # primes above 512: no kernels for these sizes
         phi = np.zeros((n, n))
         for _ in range(50):
             st = lib.esc_create(ctypes.byref(h), n, 1.0, phi.ctypes.data_as(esc._dp), ctypes.byref(cp), 0)
