@@ -266,8 +266,9 @@ def single_grid_block(name, phi, c0, steps, peak_gbs):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            ctx.run_device(d.data_ptr(), steps, DT, h.data_ptr())
+            ctx.run_device_async(d.data_ptr(), steps, DT, h.data_ptr())
             e1.record(stream)
+            ctx.wait()
             torch.cuda.synchronize()
             rates[prec] = n * n * steps / (e0.elapsed_time(e1) / 1000.0)
             out[prec] = (d.cpu().numpy(), h.cpu().numpy().reshape(6, steps + 1))
@@ -412,8 +413,11 @@ def main():
             barrier()
             torch.cuda.synchronize()
             ev0.record(stream)
-            bads = b.run_device([w.data_ptr() for w in work], steps, DT)
+            # queued without waiting: ev1 follows the join of every size group in stream
+            # order, so the interval is the device's time for exactly K steps
+            b.run_device_async([w.data_ptr() for w in work], steps, DT)
             ev1.record(stream)
+            bads = b.wait()
             torch.cuda.synchronize()
         barrier()
         ms = ev0.elapsed_time(ev1)

@@ -75,6 +75,10 @@ __global__ void k_advance(int* base, int by) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *base += by;
 }
 constexpr int kChunk = 32;  // steps per captured graph
+// Graphs are captured for chunks of 32, 16, 8, 4, 2 and 1 steps, so that any step
+// count runs as at most K/32 + 5 graph launches per group.
+constexpr int kNumChunks = 6;
+constexpr int kChunkSteps[kNumChunks] = {32, 16, 8, 4, 2, 1};
 
 struct Group {
   const esc::KernelSet* ks = nullptr;
@@ -93,7 +97,7 @@ struct Group {
   int* status = nullptr;
   long long* bad = nullptr;
   int* base = nullptr;               // this group's step counter (history row of its next step)
-  cudaGraphExec_t gexec = nullptr;   // kChunk steps of this group, captured on its own stream
+  cudaGraphExec_t gexec[kNumChunks] = {};  // kChunkSteps[i] steps of this group, captured on its own stream
   esc::InstDev* d_inst = nullptr;
   std::vector<esc::InstDev> h_inst;
   esc::ColMaps maps;      // tensor maps of S, F, G for the pipelined column kernels
@@ -160,6 +164,14 @@ bool drop_copy_knob() {
   return v && v[0] == '1';
 }
 
+// ESC_SPLIT = k: split each grid size with at least 2k particles into k groups
+// on their own streams, so that different phases of the same size overlap.
+int split_factor() {
+  const char* v = getenv("ESC_SPLIT");
+  const int k = v ? atoi(v) : 1;
+  return k >= 1 && k <= 8 ? k : 1;
+}
+
 // ESC_ROWS = warp | pipe | legacy forces one row-kernel family (measurement aid)
 int row_family_override() {
   const char* v = getenv("ESC_ROWS");
@@ -197,6 +209,10 @@ struct Engine {
   std::vector<cudaStream_t> side;    // per-group streams (their graphs, copies and tails)
   std::vector<cudaEvent_t> side_ev;  // per-group completion / join events
   cudaEvent_t fork_ev = nullptr;
+  // statuses of a device-memory run, copied back in stream order (pinned; group-major slots)
+  int* h_status = nullptr;
+  long long* h_bad = nullptr;
+  bool pending = false;  // a device-memory run was queued and not yet waited for
   std::vector<void*> allocs;
   std::string err;
   // adjoint resources (allocated on first use; single-instance contexts)
@@ -245,10 +261,15 @@ struct Engine {
   }
 
   void release() {
-    for (Group& g : groups) {
-      if (g.gexec) cudaGraphExecDestroy(g.gexec);
-      g.gexec = nullptr;
-    }
+    for (Group& g : groups)
+      for (cudaGraphExec_t& x : g.gexec) {
+        if (x) cudaGraphExecDestroy(x);
+        x = nullptr;
+      }
+    if (h_status) cudaFreeHost(h_status);
+    if (h_bad) cudaFreeHost(h_bad);
+    h_status = nullptr;
+    h_bad = nullptr;
     for (auto& kv : adj.graphs) cudaGraphExecDestroy(kv.second);
     adj.graphs.clear();
     for (int b = 0; b < 2; ++b) {
@@ -337,12 +358,20 @@ esc_status engine_create(Engine& E, int count, const int* n, const double* dx, c
     const esc_params& q = p[i];
     E.p[i] = esc::ModelParams{q.A, q.B, q.chi, q.P, q.ca, q.cb, q.cc, q.kappa, q.mobility, q.Q};
   }
-  std::map<int, int> gi;
+  // Groups: one per grid size, or, with ESC_SPLIT = k > 1, sizes with at least 2k
+  // particles split into k groups of equal size that advance on their own streams.
+  const int split = split_factor();
+  std::map<int, int> per_size;
+  for (int i = 0; i < count; ++i) ++per_size[n[i]];
+  std::map<std::pair<int, int>, int> gi;
+  std::map<int, int> seen;
   E.where.resize(count);
   for (int i = 0; i < count; ++i) {
-    auto it = gi.find(n[i]);
+    const int k = (split > 1 && per_size[n[i]] >= 2 * split) ? split : 1;
+    const int sub = seen[n[i]]++ % k;
+    auto it = gi.find({n[i], sub});
     if (it == gi.end()) {
-      it = gi.emplace(n[i], (int)E.groups.size()).first;
+      it = gi.emplace(std::make_pair(n[i], sub), (int)E.groups.size()).first;
       E.groups.emplace_back();
       E.groups.back().n = n[i];
     }
@@ -696,7 +725,7 @@ esc_status ensure_graph(Engine& E) {
       int rank = 0;
       for (int j = 0; j < ng; ++j) {
         const double wj = (double)E.groups[j].members.size() * E.groups[j].n * E.groups[j].n;
-        if (wj > work || (wj == work && j < i)) ++rank;
+        if (wj > work) ++rank;  // groups of equal work share a priority and interleave
       }
       const int prio = std::min(least, greatest + rank);
       cudaStream_t s = nullptr;
@@ -710,32 +739,50 @@ esc_status ensure_graph(Engine& E) {
   }
   for (int gi = 0; gi < ng; ++gi) {
     Group& g = E.groups[gi];
-    if (g.gexec) continue;
     cudaStream_t ss = E.side[gi];
-    cudaGraph_t graph = nullptr;
-    CK(cudaStreamBeginCapture(ss, cudaStreamCaptureModeThreadLocal));
-    for (int s = 0; s < kChunk; ++s) {
-      phase_row_a(g, g.base, s, ss);
-      phase_col_a(g, g.base, s, ss);
-      phase_row_b(g, g.base, s, ss);
-      phase_col_b(g, ss);
+    for (int ci = 0; ci < kNumChunks; ++ci) {
+      if (g.gexec[ci]) continue;
+      const int steps = kChunkSteps[ci];
+      cudaGraph_t graph = nullptr;
+      CK(cudaStreamBeginCapture(ss, cudaStreamCaptureModeThreadLocal));
+      for (int s = 0; s < steps; ++s) {
+        phase_row_a(g, g.base, s, ss);
+        phase_col_a(g, g.base, s, ss);
+        phase_row_b(g, g.base, s, ss);
+        phase_col_b(g, ss);
+      }
+      k_advance<<<1, 32, 0, ss>>>(g.base, steps);
+      const cudaError_t ec = cudaStreamEndCapture(ss, &graph);
+      if (ec != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return E.fail_cuda("cudaStreamEndCapture", ec);
+      }
+      const cudaError_t ei = cudaGraphInstantiate(&g.gexec[ci], graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess) {
+        g.gexec[ci] = nullptr;
+        return E.fail_cuda("cudaGraphInstantiate", ei);
+      }
+      // upload now, so that the first launch of a run does not carry it
+      CK(cudaGraphUpload(g.gexec[ci], ss));
     }
-    k_advance<<<1, 32, 0, ss>>>(g.base, kChunk);
-    const cudaError_t ec = cudaStreamEndCapture(ss, &graph);
-    if (ec != cudaSuccess) {
-      if (graph) cudaGraphDestroy(graph);
-      return E.fail_cuda("cudaStreamEndCapture", ec);
-    }
-    const cudaError_t ei = cudaGraphInstantiate(&g.gexec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ei != cudaSuccess) {
-      g.gexec = nullptr;
-      return E.fail_cuda("cudaGraphInstantiate", ei);
-    }
-    // upload now, so that the first launch of a run does not carry it
-    CK(cudaGraphUpload(g.gexec, ss));
     CK(cudaStreamSynchronize(ss));
   }
+  if (!E.h_status) {
+    CK(cudaMallocHost(reinterpret_cast<void**>(&E.h_status), (size_t)E.count * sizeof(int)));
+    CK(cudaMallocHost(reinterpret_cast<void**>(&E.h_bad), (size_t)E.count * sizeof(long long)));
+  }
+  return ESC_OK;
+}
+
+// Queues `steps` steps of group g on stream ss as graph launches (32-step chunks,
+// then the binary decomposition of the rest).
+esc_status launch_steps(Engine& E, Group& g, int steps, cudaStream_t ss) {
+  for (int ci = 0; ci < kNumChunks; ++ci)
+    while (steps >= kChunkSteps[ci]) {
+      CK(cudaGraphLaunch(g.gexec[ci], ss));
+      steps -= kChunkSteps[ci];
+    }
   return ESC_OK;
 }
 
@@ -744,6 +791,7 @@ esc_status ensure_graph(Engine& E) {
 // hist_dev: one device array for all instances or null.
 esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps, double dt,
                       double* const* hist_host, double* hist_dev, int64_t* bad_out, bool leave_bad_unchanged) {
+  if (E.pending) return E.fail(ESC_EINVAL, "a queued run has not been waited for");
   if (steps < 0) return E.fail(ESC_EINVAL, "steps must be >= 0");
   if (!std::isfinite(dt)) return E.fail(ESC_EINVAL, "dt must be finite");
   if (!cptr) return E.fail(ESC_EINVAL, "null composition array");
@@ -814,16 +862,7 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
         CK(cudaMemcpyAsync(g.cio + s * nn, cptr[g.members[s]], nn * sizeof(double), cudaMemcpyHostToDevice, ss));
     }
     g.ks->init(g.d_inst, cnt, ss);
-    int done = 0;
-    for (; steps - done >= kChunk; done += kChunk) CK(cudaGraphLaunch(g.gexec, ss));
-    const int rem = steps - done;
-    for (int s = 0; s < rem; ++s) {
-      phase_row_a(g, g.base, s, ss);
-      phase_col_a(g, g.base, s, ss);
-      phase_row_b(g, g.base, s, ss);
-      phase_col_b(g, ss);
-    }
-    if (rem) k_advance<<<1, 32, 0, ss>>>(g.base, rem);
+    TRY(launch_steps(E, g, steps, ss));
     // history row `steps` of the final field (no update)
     phase_row_a(g, g.base, 0, ss);
     phase_col_a(g, g.base, 0, ss);
@@ -898,6 +937,125 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
                                           (E.count > 1 ? " (instance " + std::to_string(i) + ")" : ""));
   }
   return ESC_OK;
+}
+
+// Device-memory run, queued without waiting: descriptors, fork into the groups'
+// streams, every group's steps (graph launches), final history row and final
+// field, each group's status words copied into pinned host memory, and the join
+// back into the caller's stream.  engine_wait reports the outcome.  A stopped
+// instance keeps its device c (the final-field kernel skips it).
+esc_status engine_enqueue_device(Engine& E, double* const* cptr, int steps, double dt, double* hist_dev) {
+  if (E.pending) return E.fail(ESC_EINVAL, "a queued run has not been waited for");
+  if (steps < 0) return E.fail(ESC_EINVAL, "steps must be >= 0");
+  if (!std::isfinite(dt)) return E.fail(ESC_EINVAL, "dt must be finite");
+  if (!cptr) return E.fail(ESC_EINVAL, "null composition array");
+  for (int i = 0; i < E.count; ++i)
+    if (!cptr[i]) return E.fail(ESC_EINVAL, "null composition field");
+  DeviceGuard dg(E.device);
+  const size_t rows = (size_t)steps + 1;
+  const size_t per = rows * 6;
+  double* hbase = hist_dev;
+  if (!hbase) {
+    const size_t need = per * (size_t)E.count;
+    if (need > E.hist_cap) {
+      if (E.hist) {
+        for (auto it = E.allocs.begin(); it != E.allocs.end(); ++it)
+          if (*it == E.hist) {
+            E.allocs.erase(it);
+            break;
+          }
+        cudaFree(E.hist);
+        E.hist = nullptr;
+        E.hist_cap = 0;
+      }
+      TRY(E.alloc(&E.hist, need * sizeof(double), "history"));
+      E.hist_cap = need;
+    }
+    hbase = E.hist;
+  }
+  cudaStream_t st = E.stream;
+  TRY(ensure_graph(E));
+  for (Group& g : E.groups) {
+    for (size_t s = 0; s < g.members.size(); ++s) {
+      const int i = g.members[s];
+      esc::InstDev& d = g.h_inst[s];
+      d.dt = dt;
+      d.hist = hbase + (size_t)i * per;
+      d.hist_ld = (int)rows;
+      d.cio = cptr[i];
+    }
+    CK(cudaMemcpyAsync(g.d_inst, g.h_inst.data(), g.h_inst.size() * sizeof(esc::InstDev),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(g.status, 0, g.members.size() * sizeof(int), st));
+    CK(cudaMemsetAsync(g.bad, 0xff, g.members.size() * sizeof(long long), st));
+    CK(cudaMemsetAsync(g.cnt, 0, g.members.size() * 4 * sizeof(unsigned), st));
+    CK(cudaMemsetAsync(g.base, 0, sizeof(int), st));
+  }
+  CK(cudaEventRecord(E.fork_ev, st));
+  size_t off = 0;
+  for (int gi = 0; gi < (int)E.groups.size(); ++gi) {
+    Group& g = E.groups[gi];
+    cudaStream_t ss = E.side[gi];
+    const int cnt = (int)g.members.size();
+    CK(cudaStreamWaitEvent(ss, E.fork_ev, 0));
+    g.ks->init(g.d_inst, cnt, ss);
+    TRY(launch_steps(E, g, steps, ss));
+    phase_row_a(g, g.base, 0, ss);
+    phase_col_a(g, g.base, 0, ss);
+    phase_row_b(g, g.base, 0, ss);
+    g.ks->fin(g.d_inst, cnt, ss);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(E.h_status + off, g.status, cnt * sizeof(int), cudaMemcpyDeviceToHost, ss));
+    CK(cudaMemcpyAsync(E.h_bad + off, g.bad, cnt * sizeof(long long), cudaMemcpyDeviceToHost, ss));
+    off += cnt;
+    CK(cudaEventRecord(E.side_ev[gi], ss));
+    CK(cudaStreamWaitEvent(st, E.side_ev[gi], 0));
+  }
+  E.pending = true;
+  return ESC_OK;
+}
+
+// Waits for the queued device-memory run and reports it like engine_run.
+esc_status engine_wait(Engine& E, int64_t* bad_out) {
+  if (!E.pending) return E.fail(ESC_EINVAL, "no queued run to wait for");
+  DeviceGuard dg(E.device);
+  E.pending = false;
+  CK(cudaStreamSynchronize(E.stream));
+  std::vector<int> status(E.count, 0);
+  std::vector<long long> bad(E.count, -1);
+  size_t off = 0;
+  for (const Group& g : E.groups) {
+    for (size_t k = 0; k < g.members.size(); ++k) {
+      status[g.members[k]] = E.h_status[off + k];
+      bad[g.members[k]] = E.h_bad[off + k];
+    }
+    off += g.members.size();
+  }
+  bool any_bad = false;
+  for (int i = 0; i < E.count; ++i) {
+    if (status[i]) any_bad = true;
+    if (bad_out) bad_out[i] = status[i] ? (int64_t)bad[i] : -1;
+  }
+  if (any_bad) {
+    for (int i = 0; i < E.count; ++i)
+      if (status[i] == esc::kStatusLayout)
+        return E.fail(ESC_ECUDA, "internal error: a shared-memory stage was misaligned; no copy was issued");
+    for (int i = 0; i < E.count; ++i)
+      if (status[i] == esc::kStatusTimeout)
+        return E.fail(ESC_ETIMEOUT, "a bounded wait for a tile copy gave up (instance " + std::to_string(i) + ")");
+    for (int i = 0; i < E.count; ++i)
+      if (status[i])
+        return E.fail(ESC_ENONFINITE, "Non-finite composition at step " + std::to_string(bad[i]) +
+                                          (E.count > 1 ? " (instance " + std::to_string(i) + ")" : ""));
+  }
+  return ESC_OK;
+}
+
+esc_status engine_run_device(Engine& E, double* const* cptr, int steps, double dt, double* hist_dev,
+                             int64_t* bad_out) {
+  const esc_status s = engine_enqueue_device(E, cptr, steps, dt, hist_dev);
+  if (s != ESC_OK) return s;
+  return engine_wait(E, bad_out);
 }
 
 }  // namespace
@@ -1293,7 +1451,27 @@ esc_status esc_run_device(esc_ctx* ctx, double* c, int steps, double dt, double*
   }
   double* cs[1] = {c};
   int64_t b = -1;
-  const esc_status s = engine_run(ctx->e, cs, true, steps, dt, nullptr, history, &b, true);
+  const esc_status s = engine_run_device(ctx->e, cs, steps, dt, history, &b);
+  if (bad_step) *bad_step = b;
+  return s;
+}
+
+esc_status esc_run_device_async(esc_ctx* ctx, double* c, int steps, double dt, double* history) {
+  if (!ctx) {
+    tl_err = "null context";
+    return ESC_EINVAL;
+  }
+  double* cs[1] = {c};
+  return engine_enqueue_device(ctx->e, cs, steps, dt, history);
+}
+
+esc_status esc_wait(esc_ctx* ctx, int64_t* bad_step) {
+  if (!ctx) {
+    tl_err = "null context";
+    return ESC_EINVAL;
+  }
+  int64_t b = -1;
+  const esc_status s = engine_wait(ctx->e, &b);
   if (bad_step) *bad_step = b;
   return s;
 }
@@ -1310,6 +1488,7 @@ void esc_destroy(esc_ctx* ctx) {
   if (!ctx) return;
   {
     DeviceGuard dg(ctx->e.device);
+    if (ctx->e.pending) cudaStreamSynchronize(ctx->e.stream);
     ctx->e.release();
   }
   delete ctx;
@@ -1359,7 +1538,23 @@ esc_status esc_batch_run_device(esc_batch* b, double* const* c, int steps, doubl
     tl_err = "null batch";
     return ESC_EINVAL;
   }
-  return engine_run(b->e, c, true, steps, dt, nullptr, history, bad_steps, true);
+  return engine_run_device(b->e, c, steps, dt, history, bad_steps);
+}
+
+esc_status esc_batch_run_device_async(esc_batch* b, double* const* c, int steps, double dt, double* history) {
+  if (!b) {
+    tl_err = "null batch";
+    return ESC_EINVAL;
+  }
+  return engine_enqueue_device(b->e, c, steps, dt, history);
+}
+
+esc_status esc_batch_wait(esc_batch* b, int64_t* bad_steps) {
+  if (!b) {
+    tl_err = "null batch";
+    return ESC_EINVAL;
+  }
+  return engine_wait(b->e, bad_steps);
 }
 
 esc_status esc_batch_profile_phases(esc_batch* b, int steps, int* n_groups, int* group_n, int* group_count,
@@ -1491,6 +1686,7 @@ void esc_batch_destroy(esc_batch* b) {
   if (!b) return;
   {
     DeviceGuard dg(b->e.device);
+    if (b->e.pending) cudaStreamSynchronize(b->e.stream);
     b->e.release();
   }
   delete b;

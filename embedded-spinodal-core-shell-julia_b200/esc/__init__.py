@@ -97,6 +97,8 @@ _SIGNATURES = [
     ("esc_run", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_double, _dp, _i64p]),
     ("esc_run_device", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, _vp, _i64p]),
     ("esc_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("esc_run_device_async", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, _vp]),
+    ("esc_wait", ctypes.c_int, [_vp, _i64p]),
     ("esc_last_error", ctypes.c_char_p, [_vp]),
     ("esc_destroy", None, [_vp]),
     ("esc_adjoint", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_int,
@@ -108,6 +110,8 @@ _SIGNATURES = [
     ("esc_batch_run_device", ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double,
                                             _vp, _i64p]),
     ("esc_batch_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("esc_batch_run_device_async", ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double, _vp]),
+    ("esc_batch_wait", ctypes.c_int, [_vp, _i64p]),
     ("esc_batch_adjoint", ctypes.c_int, [_vp, ctypes.POINTER(_dp), ctypes.c_int, ctypes.c_double,
                                          ctypes.POINTER(_dp), ctypes.c_double, ctypes.c_int, ctypes.POINTER(_dp),
                                          _dp, _dp]),
@@ -252,6 +256,20 @@ class Context:
         if st != ESC_OK:
             _raise(st, self._err(), bad.value)
 
+    def run_device_async(self, c_ptr: int, steps: int, dt: float, hist_ptr: int = 0) -> None:
+        """esc_run_device_async: queues the run on the context's stream and returns; call wait()."""
+        st = load_library().esc_run_device_async(self._h, _vp(c_ptr), int(steps), float(dt),
+                                                 _vp(hist_ptr) if hist_ptr else None)
+        if st != ESC_OK:
+            _raise(st, self._err())
+
+    def wait(self) -> None:
+        """esc_wait: waits for the queued run; raises NonFiniteError like run_device."""
+        bad = ctypes.c_int64(-1)
+        st = load_library().esc_wait(self._h, ctypes.byref(bad))
+        if st != ESC_OK:
+            _raise(st, self._err(), bad.value)
+
     def set_stream(self, stream_ptr: int) -> None:
         st = load_library().esc_set_stream(self._h, _vp(stream_ptr) if stream_ptr else None)
         if st != ESC_OK:
@@ -326,6 +344,22 @@ class Batch:
         bad = (ctypes.c_int64 * self.count)()
         st = load_library().esc_batch_run_device(self._h, carr, int(steps), float(dt),
                                                  _vp(hist_ptr) if hist_ptr else None, bad)
+        if st not in (ESC_OK, ESC_ENONFINITE):
+            _raise(st, self._err())
+        return [int(b) for b in bad]
+
+    def run_device_async(self, c_ptrs: Sequence[int], steps: int, dt: float, hist_ptr: int = 0) -> None:
+        """esc_batch_run_device_async: queues the run on the batch's stream and returns; call wait()."""
+        carr = (_vp * self.count)(*[_vp(p) for p in c_ptrs])
+        st = load_library().esc_batch_run_device_async(self._h, carr, int(steps), float(dt),
+                                                       _vp(hist_ptr) if hist_ptr else None)
+        if st != ESC_OK:
+            _raise(st, self._err())
+
+    def wait(self):
+        """esc_batch_wait: waits for the queued run; returns the per-instance bad steps like run_device."""
+        bad = (ctypes.c_int64 * self.count)()
+        st = load_library().esc_batch_wait(self._h, bad)
         if st not in (ESC_OK, ESC_ENONFINITE):
             _raise(st, self._err())
         return [int(b) for b in bad]

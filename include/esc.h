@@ -88,6 +88,19 @@ esc_status esc_run(esc_ctx *ctx, double *c, int steps, double dt, double *histor
  * call returns when it has finished. */
 esc_status esc_run_device(esc_ctx *ctx, double *c, int steps, double dt, double *history, int64_t *bad_step);
 
+/* Queues the work of esc_run_device on the context's stream and returns without
+ * waiting: an event the caller records on that stream afterwards completes with
+ * the run, so the run can be timed on the device alone.  esc_wait must follow
+ * before c or the history is read and before any other call on the context (a
+ * second run before it returns ESC_EINVAL).  Argument errors are reported here;
+ * the outcome of the run (ESC_ENONFINITE and the step, ESC_ETIMEOUT) by esc_wait.
+ * No counterpart in the reference. */
+esc_status esc_run_device_async(esc_ctx *ctx, double *c, int steps, double dt, double *history);
+
+/* Waits for the run queued by esc_run_device_async and reports it as esc_run_device
+ * would (*bad_step = -1 or the step of a non-finite field). */
+esc_status esc_wait(esc_ctx *ctx, int64_t *bad_step);
+
 /* Uses `stream` (a cudaStream_t) for all later work of the context; NULL restores
  * the context's own stream. */
 esc_status esc_set_stream(esc_ctx *ctx, void *stream);
@@ -128,6 +141,13 @@ esc_status esc_batch_run(esc_batch *b, double *const *c, int steps, double dt, d
  * of count*(steps+1)*6 doubles, instance i at offset i*(steps+1)*6. */
 esc_status esc_batch_run_device(esc_batch *b, double *const *c, int steps, double dt, double *history,
                                 int64_t *bad_steps);
+
+/* esc_batch_run_device split in two, as esc_run_device_async / esc_wait: the first
+ * queues the whole run (the fork into the size groups' streams, their graph
+ * launches, and the join back into the batch's stream) and returns at once; the
+ * second waits and reports the outcome (bad_steps, count entries, may be NULL). */
+esc_status esc_batch_run_device_async(esc_batch *b, double *const *c, int steps, double dt, double *history);
+esc_status esc_batch_wait(esc_batch *b, int64_t *bad_steps);
 
 esc_status esc_batch_set_stream(esc_batch *b, void *stream);
 
