@@ -254,7 +254,9 @@ def single_grid_block(name, phi, c0, steps, peak_gbs):
     import torch
     import esc
     n = phi.shape[0]
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the queued run and the events bracketing it share it
+    # (a null handle would leave the context on its own stream, outside the events)
+    stream = torch.cuda.Stream()
     rates, out = {}, {}
     for prec in ("fp64", "mixed"):
         with esc.Context(phi, precision=prec) as ctx:
