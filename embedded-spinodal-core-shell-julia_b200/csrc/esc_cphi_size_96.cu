@@ -1,0 +1,4 @@
+// Coupled c-phi kernel set for axis length 96 (FP64).
+#include "esc_cphi.cuh"
+
+ESC_CPHI_DEFINE_SIZE(96)

@@ -37,9 +37,9 @@ FP64 = 0
 MIXED = 1
 _PREC = {"fp64": FP64, "mixed": MIXED, FP64: FP64, MIXED: MIXED}
 
-ESC_OK, ESC_EINVAL, ESC_ECUDA, ESC_ENONFINITE, ESC_ETIMEOUT, ESC_ENOMEM = range(6)
+ESC_OK, ESC_EINVAL, ESC_ECUDA, ESC_ENONFINITE, ESC_ETIMEOUT, ESC_ENOMEM, ESC_EMASS = range(7)
 _STATUS_NAMES = {0: "ESC_OK", 1: "ESC_EINVAL", 2: "ESC_ECUDA", 3: "ESC_ENONFINITE",
-                 4: "ESC_ETIMEOUT", 5: "ESC_ENOMEM"}
+                 4: "ESC_ETIMEOUT", 5: "ESC_ENOMEM", 6: "ESC_EMASS"}
 
 
 @dataclasses.dataclass(frozen=True)
@@ -81,6 +81,12 @@ class _CParams(ctypes.Structure):
     @classmethod
     def of(cls, p: Parameters) -> "_CParams":
         return cls(*[float(getattr(p, f)) for f, _ in cls._fields_])
+
+
+class _CCphiParams(ctypes.Structure):
+    """esc_cphi_params: constants of the coupled c-phi model (original/2023-3d/InputParams:13-22)."""
+    _fields_ = [(f, ctypes.c_double) for f in
+                ("A", "B", "chi", "P", "ca", "cb1", "cb2", "A0", "kappa_c", "kappa_phi", "mobility", "relax", "Q")]
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -126,6 +132,18 @@ _SIGNATURES = [
     ("esc_julia_rand", ctypes.c_int, [ctypes.c_uint64, _dp, ctypes.c_int64]),
     ("esc_batch_last_error", ctypes.c_char_p, [_vp]),
     ("esc_batch_destroy", None, [_vp]),
+    ("esc_cphi_default_params", None, [ctypes.POINTER(_CCphiParams)]),
+    ("esc_cphi_supported_size", ctypes.c_int, [ctypes.c_int]),
+    ("esc_cphi_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.POINTER(_CCphiParams)]),
+    ("esc_cphi_run", ctypes.c_int, [_vp, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    _dp, _i64p, ctypes.POINTER(ctypes.c_int)]),
+    ("esc_cphi_run_device", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double, _vp, _i64p, ctypes.POINTER(ctypes.c_int)]),
+    ("esc_cphi_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("esc_cphi_last_error", ctypes.c_char_p, [_vp]),
+    ("esc_cphi_destroy", None, [_vp]),
 ]
 
 _LIB: Optional[ctypes.CDLL] = None

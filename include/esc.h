@@ -48,7 +48,9 @@ typedef enum {
   ESC_ECUDA = 2,       /* CUDA runtime error (message in esc_last_error) */
   ESC_ENONFINITE = 3,  /* composition became non-finite (core_shell.jl:93); *bad_step holds s */
   ESC_ETIMEOUT = 4,    /* a bounded device-side wait gave up */
-  ESC_ENOMEM = 5       /* device allocation failed */
+  ESC_ENOMEM = 5,      /* device allocation failed */
+  ESC_EMASS = 6        /* coupled model: the mean composition moved by more than comperr in one step
+                          (original/2023-3d/evolve.cu:145-155) */
 } esc_status;
 
 typedef enum {
@@ -244,6 +246,69 @@ esc_status esc_julia_rand(uint64_t seed, double *out, int64_t count);
 esc_status esc_run_noalloc(int n, double dx, const double *phi, const esc_params *p, double *c, int steps,
                            double dt, double *history, int64_t *bad_step, void *stream);
 void esc_batch_destroy(esc_batch *b);
+
+/* ---- Coupled c-phi model (3-D) ------------------------------------------------------------
+ * Conserved composition c (Cahn-Hilliard, variable mobility M = mobility h(phi)) coupled to
+ * an order parameter phi that relaxes by Allen-Cahn dynamics: the step of the reference's
+ * 2023 3-D program (original/2023-3d/evolve.cu:86-186, kernels original/2023-3d/EvoKernels.h).
+ * Per step: df/dc and df/dphi of f(c, phi) = (1-h)(A(c-ca)^2 + A0) + h B (c-cb1)^2 (c-cb2)^2
+ * + P (1 - chi c) g; mu^ = FFT(df/dc) + 2 kappa_c k^2 c^; div = sum_a D_a(M D_a mu) with the
+ * fourth-order central difference D_a; c^ <- (dt div^ + lhs c^)/lhs, lhs = 1 + 2 Q kappa_c k^4 dt;
+ * phi^ <- (phi^ - relax dt FFT(df/dphi)) / (1 + 2 relax kappa_phi k^2 dt).  FP64 throughout.
+ * The z-gradient of mu uses dz (the reference passes dy there, evolve.cu:124).
+ * Fields are nx*ny*nz real arrays in the reference's order a[k + nz*(j + ny*i)] (z
+ * contiguous).  Each of nx, ny, nz must be one of 8, 12, 16, 24, 32, 48, 64, 96, 128, 192,
+ * 256, 384, 512 (esc_cphi_supported_size). */
+typedef struct {
+  double A, B, chi, P, ca, cb1, cb2, A0, kappa_c, kappa_phi, mobility, relax, Q;
+} esc_cphi_params;
+typedef struct esc_cphi esc_cphi;
+
+/* stop reasons reported by esc_cphi_run */
+#define ESC_CPHI_COMPLETED 0    /* all steps ran */
+#define ESC_CPHI_CONVERGED 1    /* max|c - c_prev| <= tolerance after a step (evolve.cu:168-181) */
+#define ESC_CPHI_OUT_OF_BOUNDS 2 /* some c < -0.4 or c > 1.4 after a step (EvoKernels.h:489-508) */
+#define ESC_CPHI_MASS_ERROR 3   /* mean composition drift > comperr (returns ESC_EMASS) */
+#define ESC_CPHI_NONFINITE 4    /* non-finite c or phi (returns ESC_ENONFINITE) */
+
+/* Fills p with the constants of original/2023-3d/InputParams:13-22
+ * (A=2, B=1, chi=0.5, P=6, ca=0.5, cb1=0, cb2=1, A0=0.08, kappa_c=2, kappa_phi=10,
+ * mobility=1, relax=0.001, Q=0.5). */
+void esc_cphi_default_params(esc_cphi_params *p);
+
+/* 1 if n is a supported size of one axis of the coupled model, else 0. */
+int esc_cphi_supported_size(int n);
+
+/* Creates a coupled-model context for an nx x ny x nz grid with spacings dx, dy, dz.
+ * Replaces the set-up of original/2023-3d/main.cu:80-110 (k-vectors, plans). */
+esc_status esc_cphi_create(esc_cphi **out, int nx, int ny, int nz, double dx, double dy, double dz,
+                           const esc_cphi_params *p);
+
+/* Runs up to `steps` steps from (c, phi) (host arrays, in/out), the loop of
+ * original/2023-3d/evolve.cu:74-186.  history ((steps+1) x 6 column-major, may be NULL)
+ * gets row s = [s*dt, mean c, mean phi, min c, max c, max|c_s - c_(s-1)|] for the fields
+ * after s steps (row 0: the input, last column 0); rows after the last step run stay 0.
+ * The run ends early when max|c - c_prev| <= tolerance (tolerance 0: never, unless c stops
+ * changing), when c leaves [-0.4, 1.4] (both return ESC_OK with the fields after that
+ * step), when the mean composition of c^'s k = 0 mode moves from the input mean by more
+ * than comperr (1e-8 in the reference; returns ESC_EMASS with the fields before the
+ * failing step), or on a non-finite value (ESC_ENONFINITE, fields of that step).
+ * *steps_done gets the number of steps whose fields are returned, *stop_reason one of
+ * ESC_CPHI_*. */
+esc_status esc_cphi_run(esc_cphi *ctx, double *c, double *phi, int steps, double dt, double tolerance,
+                        double comperr, double *history, int64_t *steps_done, int *stop_reason);
+
+/* esc_cphi_run with DEVICE arrays c, phi and history (history may be NULL). */
+esc_status esc_cphi_run_device(esc_cphi *ctx, double *c, double *phi, int steps, double dt, double tolerance,
+                               double comperr, double *history, int64_t *steps_done, int *stop_reason);
+
+/* Queues later runs on `stream` (a cudaStream_t; NULL = the context's own stream). */
+esc_status esc_cphi_set_stream(esc_cphi *ctx, void *stream);
+
+/* Message of the context's last failure (esc_last_error(NULL) for a failed creation). */
+const char *esc_cphi_last_error(const esc_cphi *ctx);
+
+void esc_cphi_destroy(esc_cphi *ctx);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from oracle import core_shell_oracle as orc  # noqa: E402
+from oracle import coupled_oracle as cpl  # noqa: E402
 
 CASES = [
     # name, n, radius, width, seed, steps, dt, params overrides
@@ -34,7 +35,22 @@ def make(name, n, radius, width, seed, steps, dt, over):
                         params=np.array(p.as_tuple()), dt=dt, steps=steps)
 
 
+def make_coupled():
+    """The coupled c-phi model (original/2023-3d restated): a 24 x 16 x 32 grid with
+    unequal spacings and non-default constants, 25 steps."""
+    p = cpl.CoupledParameters(P=5.0, kappa_phi=6.0, relax=0.01, A0=0.1)
+    c0, phi0 = cpl.initial_fields(24, 16, 32, 6.0, seed=7, p=p)
+    spacing = (1.0, 0.9, 1.1)
+    c, phi, hist, done, reason = cpl.run(c0, phi0, p, 0.01, 25, spacing=spacing)
+    names = list(vars(p).keys())
+    np.savez_compressed(os.path.join(HERE, "coupled_24x16x32.npz"), c0=c0, phi0=phi0, c=c, phi=phi, history=hist,
+                        param_names=np.array(names), param_values=np.array([vars(p)[k] for k in names]),
+                        dt=0.01, steps=25, spacing=np.array(spacing))
+
+
 if __name__ == "__main__":
     for case in CASES:
         make(*case)
         print("wrote", case[0])
+    make_coupled()
+    print("wrote coupled_24x16x32")

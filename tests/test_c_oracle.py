@@ -67,7 +67,7 @@ def test_c_oracle_spacing_and_whole_field_noise():
     assert hist_rel(h1, h2) < RTOL
 
 
-@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "disc*.npz"))))
 def test_c_oracle_reproduces_golden_fixtures(path):
     g = np.load(path)
     p = orc.Parameters(*[float(x) for x in g["params"]])
