@@ -302,6 +302,71 @@ def large_grid_configs(peak_gbs):
             single_grid_block("4096^2 ellipse 1600x1200, 10000 steps", phi5, c05, 10000, peak_gbs)]
 
 
+def coupled_kernel_bytes(nx, ny, nz):
+    """Bytes each of the twelve kernels of a coupled step must move (FP64: real fields 8 B
+    per point, half spectra 16 B per mode, nx*ny*(nz/2+1) modes), in launch order."""
+    n3 = nx * ny * nz
+    nk = nx * ny * (nz // 2 + 1)
+    return [16 * n3 + 32 * nk, 64 * nk, 96 * nk, 32 * nk, 16 * nk + 24 * n3, 32 * n3, 32 * n3,
+            8 * n3 + 16 * nk, 32 * nk, 96 * nk, 64 * nk, 32 * nk + 24 * n3]
+
+
+def coupled_block(peak_gbs, steps=20, warmup=3, cpu=True):
+    """The coupled c-phi model of the reference's 3-D program at its own input size
+    (original/2023-3d/InputParams: 256^3, dx = 1, dt = 0.01, R = 70, c_0 = 0.5, noise 0.05,
+    the InputParams constants), FP64, fields resident in HBM (esc_cphi_run_device), CUDA
+    events around `steps` steps on the context's stream; per-kernel times of one step
+    (esc_cphi_profile) with each kernel's bytes and fraction of the HBM peak; and the
+    CPU oracle (NumPy/scipy.fft restatement) on a 64^3 sample."""
+    import torch
+    from esc import coupled
+    shape = (256, 256, 256)
+    c0, phi0 = coupled.initial_fields(*shape, 70.0)
+    n3 = int(np.prod(shape))
+    stream = torch.cuda.Stream()
+    with coupled.Coupled(shape) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        dc, dp = torch.from_numpy(c0).cuda(), torch.from_numpy(phi0).cuda()
+        torch.cuda.synchronize()
+        ctx.run_device(dc.data_ptr(), dp.data_ptr(), warmup, DT)
+        dc.copy_(torch.from_numpy(c0))
+        dp.copy_(torch.from_numpy(phi0))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        done, reason = ctx.run_device(dc.data_ptr(), dp.data_ptr(), steps, DT)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        prof = ctx.profile(steps=3)
+    rate = n3 * steps / (ms / 1000.0)
+    nbytes = coupled_kernel_bytes(*shape)
+    kernels = []
+    for (name, kms), b in zip(prof.items(), nbytes):
+        kernels.append({"kernel": name, "ms": round(kms, 4), "bytes": b,
+                        "frac_of_hbm_peak": b / (kms / 1000.0) / (peak_gbs * 1e9)})
+    dom = max(kernels, key=lambda k: k["ms"])
+    step_bytes = sum(nbytes) / n3
+    out = {"workload": "coupled c-phi 256^3 (original/2023-3d InputParams), FP64, dt=0.01",
+           "steps": steps, "steps_done": done, "stop_reason": reason, "pt_steps_per_s": rate,
+           "ms_per_step": ms / steps, "bytes_per_pt_step": step_bytes,
+           "step_frac_of_hbm_peak": rate * step_bytes / (peak_gbs * 1e9),
+           "dominant_kernel": dom, "kernels": kernels}
+    if cpu:
+        from oracle import coupled_oracle as cpl
+        import scipy.fft as sfft
+        cs, ps_ = cpl.initial_fields(64, 64, 64, 17.5)
+        workers = os.cpu_count() or 1
+        with sfft.set_workers(workers):
+            cpl.run(cs, ps_, cpl.CoupledParameters(), DT, 1)
+            t0 = time.perf_counter()
+            cpl.run(cs, ps_, cpl.CoupledParameters(), DT, 5)
+            tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 64 ** 3 * 5 / tc, "unit": UNIT, "cores": workers, "kind": "port",
+                               "sample": "64^3 x 5 steps of the NumPy/scipy.fft restatement of the 3-D loop"}
+    return out
+
+
 def batched_gradient_block(count=64, n=512, steps=1000):
     """Batched parameter-fit gradients: `count` particles at n^2 (disc R ~ U(0.25, 0.42) n,
     w = 2, sampled P, chi, kappa as in the ensemble), loss 1/2 |c_T - c_target|^2 + 1e-3 F[c_T]
@@ -360,6 +425,9 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=2000)
     ap.add_argument("--no-large", action="store_true", help="skip the 1024^2 and 4096^2 single-grid runs")
+    ap.add_argument("--no-coupled", action="store_true", help="skip the coupled c-phi 256^3 leg")
+    ap.add_argument("--coupled-only", action="store_true",
+                    help="run only the coupled c-phi 256^3 leg and print its JSON object")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -374,6 +442,10 @@ def main():
     import torch
     import esc
     torch.cuda.set_device(local)
+    if args.coupled_only:
+        print(json.dumps(coupled_block(read_peaks()[0], steps=args.steps, warmup=args.warmup,
+                                       cpu=not args.no_cpu)), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -540,6 +612,9 @@ def main():
     batched_grad = None
     if not args.no_adjoint:
         batched_grad = batched_gradient_block()
+    coupled_leg = None
+    if not args.no_coupled:
+        coupled_leg = coupled_block(peak, cpu=(rank == 0 and world == 1 and not args.no_cpu))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -575,7 +650,7 @@ def main():
         "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
         "fp64_dropin": fp64, "max_abs_err_vs_fp64": max_err, "accuracy": accuracy, "large_grids": large,
         "clocks": clocks,
-        "adjoint": adjoint, "batched_gradients": batched_grad,
+        "adjoint": adjoint, "batched_gradients": batched_grad, "coupled": coupled_leg,
         "nonfinite_instances": int(sum(1 for x in bads if x >= 0)),
         "kernel_families": tuned,
     }

@@ -41,6 +41,13 @@ __global__ void __launch_bounds__(kBlock) k3_fd_line(const Dev* __restrict__ dp,
   double* qt = mt + (size_t)n * kFdW;
   const int total = n * kFdW;
   const double inv12 = 1.0 / (12.0 * h);
+  // neighbour rows p +- 1, p +- 2 with the periodic wrap, without a runtime modulo
+  auto row = [n](int p, int o) {
+    int r = p + o;
+    r += (r < 0) ? n : 0;
+    r -= (r >= n) ? n : 0;
+    return r * kFdW;
+  };
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int p = idx / kFdW, w = idx % kFdW;
     mt[idx] = (k0 + w < d.nz) ? d.mu[base + (long)p * estride + w] : 0.0;
@@ -48,18 +55,34 @@ __global__ void __launch_bounds__(kBlock) k3_fd_line(const Dev* __restrict__ dp,
   __syncthreads();
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int p = idx / kFdW, w = idx % kFdW;
-    const double dm = fd4(mt[((p + 2) % n) * kFdW + w], mt[((p + 1) % n) * kFdW + w],
-                          mt[((p + n - 1) % n) * kFdW + w], mt[((p + n - 2) % n) * kFdW + w], inv12);
+    const double dm = fd4(mt[row(p, 2) + w], mt[row(p, 1) + w], mt[row(p, -1) + w], mt[row(p, -2) + w], inv12);
     const double M = (k0 + w < d.nz) ? mobility3(d.phi[base + (long)p * estride + w], d.p.mobility) : 0.0;
     qt[idx] = M * dm;
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int p = idx / kFdW, w = idx % kFdW;
-    if (k0 + w >= d.nz) continue;
-    const double dq = fd4(qt[((p + 2) % n) * kFdW + w], qt[((p + 1) % n) * kFdW + w],
-                          qt[((p + n - 1) % n) * kFdW + w], qt[((p + n - 2) % n) * kFdW + w], inv12);
-    d.div[base + (long)p * estride + w] += dq;
+  // div += D q, four points per thread at a time: their div loads are issued
+  // together, ahead of the stores (which the compiler may not move loads across)
+  constexpr int U = 4;
+  for (int i0 = threadIdx.x; i0 < total; i0 += U * blockDim.x) {
+    double old[U];
+    long at[U];
+    bool ok[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = i0 + u * blockDim.x;
+      const int p = idx / kFdW, w = idx % kFdW;
+      ok[u] = idx < total && k0 + w < d.nz;
+      at[u] = base + (long)p * estride + w;
+      old[u] = ok[u] ? d.div[at[u]] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!ok[u]) continue;
+      const int idx = i0 + u * blockDim.x;
+      const int p = idx / kFdW, w = idx % kFdW;
+      const double dq = fd4(qt[row(p, 2) + w], qt[row(p, 1) + w], qt[row(p, -1) + w], qt[row(p, -2) + w], inv12);
+      d.div[at[u]] = old[u] + dq;
+    }
   }
 }
 
@@ -216,8 +239,11 @@ std::mutex& cphi_mutex() {
   return m;
 }
 
-// One step of the coupled model (twelve launches), s_local its index inside the chunk.
-void launch_step(esc_cphi& X, int s_local, cudaStream_t st) {
+// One step of the coupled model (twelve launches), s_local its index inside the
+// chunk.  With `ev` (13 events), ev[k] is recorded before launch k and ev[12]
+// after the last (per-kernel timing).
+constexpr int kStepKernels = 12;
+void launch_step(esc_cphi& X, int s_local, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   using namespace esc::cphi;
   const Dev* d = X.d_dev;
   const long L = (long)X.nx * X.ny;
@@ -226,20 +252,36 @@ void launch_step(esc_cphi& X, int s_local, cudaStream_t st) {
   const dim3 gy((X.K + X.sy->lW - 1) / X.sy->lW, X.nx);  // y lines (i, kz)
   const dim3 gx((X.K + X.sx->lW - 1) / X.sx->lW, X.ny);  // x lines (j, kz)
   const long ey = X.K, oy = (long)X.ny * X.K;
-  const long ex = (long)X.ny * X.K, ox = X.K;
   const dim3 gfy((X.nz + kFdW - 1) / kFdW, X.nx), gfx((X.nz + kFdW - 1) / kFdW, X.ny);
+  int k = 0;
+  auto mark = [&]() {
+    if (ev) cudaEventRecord(ev[k++], st);
+  };
+  mark();
   X.sz->zf(d, kZLocal, zb_line, st);
+  mark();
   X.sy->line(d, false, X.h.D1, X.h.D2, 2, ey, oy, gy, st);
+  mark();
   X.sx->xspec(d, kXMu, s_local, gx, st);
+  mark();
   X.sy->line(d, true, X.h.D1, nullptr, 1, ey, oy, gy, st);
+  mark();
   X.sz->zi_mu(d, zb_pair, st);
+  mark();
   k3_fd_line<<<gfy, esc::kBlock, (size_t)2 * X.ny * kFdW * sizeof(double), st>>>(d, 1);
+  mark();
   k3_fd_line<<<gfx, esc::kBlock, (size_t)2 * X.nx * kFdW * sizeof(double), st>>>(d, 0);
+  mark();
   X.sz->zf(d, kZDiv, zb_pair, st);
+  mark();
   X.sy->line(d, false, X.h.D1, nullptr, 1, ey, oy, gy, st);
+  mark();
   X.sx->xspec(d, kXUpdate, s_local, gx, st);
+  mark();
   X.sy->line(d, true, X.h.D1, X.h.D2, 2, ey, oy, gy, st);
+  mark();
   X.sz->zi_final(d, s_local, zb_line, st);
+  mark();
 }
 
 esc_status ensure_graphs(esc_cphi& X) {
@@ -502,6 +544,44 @@ esc_status esc_cphi_run_device(esc_cphi* ctx, double* c, double* phi, int steps,
     return ESC_EINVAL;
   }
   return run_impl(*ctx, c, phi, true, steps, dt, tolerance, comperr, history, steps_done, stop_reason);
+}
+
+esc_status esc_cphi_profile(esc_cphi* ctx, int steps, double* ms) {
+  if (!ctx || steps < 1 || !ms) {
+    esc_set_thread_error("bad argument");
+    return ESC_EINVAL;
+  }
+  esc_cphi& X = *ctx;
+  if (!X.hist) return X.fail(ESC_EINVAL, "profile needs a previous run (it steps the fields that run left)");
+  Guard dg(X.device);
+  cudaStream_t st = X.stream;
+  // step on from the last run's fields: no early stop, history into row 0 of the library's buffer
+  X.h.tol = -1.0;
+  X.h.comperr = INFINITY;
+  X.h.hist_ld = 1;
+  CK(cudaMemcpyAsync(X.d_dev, &X.h, sizeof(Dev), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(X.status, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(X.base, 0, sizeof(int), st));
+  cudaEvent_t ev[kStepKernels + 1];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  std::vector<double> acc(kStepKernels, 0.0);
+  esc_status rs = ESC_OK;
+  for (int s = 0; s < steps && rs == ESC_OK; ++s) {
+    CK(cudaMemsetAsync(X.base, 0, sizeof(int), st));
+    launch_step(X, 0, st, ev);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[kStepKernels]);
+    for (int k = 0; k < kStepKernels && e == cudaSuccess; ++k) {
+      float t = 0.f;
+      e = cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+    if (e != cudaSuccess) rs = X.fail_cuda("profile", e);
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (rs != ESC_OK) return rs;
+  for (int k = 0; k < kStepKernels; ++k) ms[k] = acc[k] / steps;
+  return ESC_OK;
 }
 
 const char* esc_cphi_last_error(const esc_cphi* ctx) { return ctx ? ctx->err.c_str() : esc_last_error(nullptr); }

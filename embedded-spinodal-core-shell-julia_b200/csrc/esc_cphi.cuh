@@ -119,8 +119,14 @@ struct ZGeom {
 
 // forward z transforms.  kZInit: (c + i phi) of line q -> D1 = c^, D2 = phi^;
 // kZLocal: (df/dc + i df/dphi) of line q -> D1, D2; kZDiv: div of lines 2q, 2q+1 -> D1.
+// resident 256-thread blocks per SM the coupled kernels are compiled for
 template <class P>
-__global__ void __launch_bounds__(kBlock) k3_zf(const Dev* __restrict__ dp, int mode) {
+constexpr int cphi_minb() {
+  return P::E <= 8 ? 2 : 1;
+}
+
+template <class P>
+__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zf(const Dev* __restrict__ dp, int mode) {
   using ZG = ZGeom<P>;
   constexpr int N = ZG::N, E = ZG::E, T = ZG::T, G = ZG::G, K = ZG::K;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -175,7 +181,7 @@ __global__ void __launch_bounds__(kBlock) k3_zf(const Dev* __restrict__ dp, int 
 // inverse z transform of mu^ (lines 2q, 2q+1 of D1 in one complex FFT), then the
 // z part of div: D_z(M D_z mu) along the line; writes mu and div
 template <class P>
-__global__ void __launch_bounds__(kBlock) k3_zi_mu(const Dev* __restrict__ dp) {
+__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_mu(const Dev* __restrict__ dp) {
   using ZG = ZGeom<P>;
   constexpr int N = ZG::N, E = ZG::E, T = ZG::T, G = ZG::G, K = ZG::K;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -198,8 +204,13 @@ __global__ void __launch_bounds__(kBlock) k3_zi_mu(const Dev* __restrict__ dp) {
   const double inv12 = 1.0 / (12.0 * d.dz);
 #pragma unroll
   for (int m = 0; m < E; ++m) {
+    const int x = t + T * m;
     v[m] = cscale(v[m], d.invN);
-    sm[lay(t + T * m)] = v[m];
+    sm[lay(x)] = v[m];
+    if (active) {
+      d.mu[la * N + x] = v[m].x;
+      if (hasb) d.mu[(la + 1) * N + x] = v[m].y;
+    }
   }
   __syncthreads();
   // q = M D_z mu at this thread's points (lane x: line a, lane y: line b)
@@ -227,12 +238,8 @@ __global__ void __launch_bounds__(kBlock) k3_zi_mu(const Dev* __restrict__ dp) {
     const int x = t + T * m;
     const cpx<double> p2 = sm[lay((x + 2) % N)], p1 = sm[lay((x + 1) % N)];
     const cpx<double> m1 = sm[lay((x + N - 1) % N)], m2 = sm[lay((x + N - 2) % N)];
-    d.mu[la * N + x] = v[m].x;
     d.div[la * N + x] = fd4(p2.x, p1.x, m1.x, m2.x, inv12);
-    if (hasb) {
-      d.mu[(la + 1) * N + x] = v[m].y;
-      d.div[(la + 1) * N + x] = fd4(p2.y, p1.y, m1.y, m2.y, inv12);
-    }
+    if (hasb) d.div[(la + 1) * N + x] = fd4(p2.y, p1.y, m1.y, m2.y, inv12);
   }
 }
 
@@ -303,7 +310,7 @@ __device__ __forceinline__ bool six_fold(const Six& mine, double* part, unsigned
 
 // inverse z transform of (c^' + i phi^') per line -> c, phi; history row and stop checks
 template <class P>
-__global__ void __launch_bounds__(kBlock) k3_zi_final(const Dev* __restrict__ dp, int s_local) {
+__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_final(const Dev* __restrict__ dp, int s_local) {
   using ZG = ZGeom<P>;
   constexpr int N = ZG::N, E = ZG::E, T = ZG::T, G = ZG::G, K = ZG::K;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -315,28 +322,37 @@ __global__ void __launch_bounds__(kBlock) k3_zi_final(const Dev* __restrict__ dp
   const long L = (long)d.nx * d.ny;
   const long l = (long)blockIdx.x * G + g;
   const bool active = l < L;
+  // the previous c is loaded beside the spectra, before the transform: the stores
+  // below go to the same addresses, and loads issued after them would each wait
+  // for a full memory round trip in turn
+  double* __restrict__ cp = d.c + l * N;
+  double* __restrict__ pp = d.phi + l * N;
   cpx<double> v[E];
+  double co[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m)
+  for (int m = 0; m < E; ++m) {
     v[m] = active ? merge_half<N>(d.D1 + l * K, d.D2 + l * K, t + T * m) : mkc<double>(0.0, 0.0);
+    co[m] = active ? cp[t + T * m] : 0.0;
+  }
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
   const RowLayout<N> lay{g * RowLayout<N>::stride};
   fft<true, P>(v, t, sm, lay, PassTable<P, double>{});
   Six s = six_identity();
   if (active) {
     int nbad = 0;
+    const double invN = d.invN;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
-      const long o = l * N + t + T * m;
-      const double cn = v[m].x * d.invN, pn = v[m].y * d.invN;
-      const double co = d.c[o];
-      d.c[o] = cn;
-      d.phi[o] = pn;
+      const int o = t + T * m;
+      const double cn = v[m].x * invN, pn = v[m].y * invN;
+      const double co_ = co[m];
+      cp[o] = cn;
+      pp[o] = pn;
       s.v[0] += cn;
       s.v[1] += pn;
       s.v[2] = fmin(s.v[2], cn);
       s.v[3] = fmax(s.v[3], cn);
-      s.v[4] = fmax(s.v[4], fabs(cn - co));
+      s.v[4] = fmax(s.v[4], fabs(cn - co_));
       nbad += (int)(nonfinite_bits(cn) | nonfinite_bits(pn));
     }
     s.v[5] = (double)nbad;
@@ -378,7 +394,7 @@ struct LGeom {
 // in-place transforms of na (1 or 2) arrays along a strided axis: element p of
 // line (o, kz) at o*ostride + kz + p*estride
 template <class P, bool INV>
-__global__ void __launch_bounds__(kBlock) k3_line(const Dev* __restrict__ dp, double2* a0, double2* a1, int na,
+__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_line(const Dev* __restrict__ dp, double2* a0, double2* a1, int na,
                                                   long estride, long ostride) {
   using LG = LGeom<P>;
   constexpr int E = LG::E, T = LG::T, W = LG::W;
@@ -411,7 +427,7 @@ __global__ void __launch_bounds__(kBlock) k3_line(const Dev* __restrict__ dp, do
 enum XOp { kXInit = 0, kXMu = 1, kXUpdate = 2 };
 
 template <class P, int OP>
-__global__ void __launch_bounds__(kBlock) k3_xspec(const Dev* __restrict__ dp, int s_local) {
+__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __restrict__ dp, int s_local) {
   using LG = LGeom<P>;
   constexpr int N = LG::N, E = LG::E, T = LG::T, W = LG::W;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -494,13 +510,13 @@ __global__ void __launch_bounds__(kBlock) k3_xspec(const Dev* __restrict__ dp, i
       const double k2 = k2_at(p);
       const double lhs = 1.0 + c1 * k2 * k2;
       v[m] = mkc<double>((d.dt * v[m].x + lhs * ch.x) / lhs, (d.dt * v[m].y + lhs * ch.y) / lhs);
-      if (p == 0 && j == 0 && kz == 0) {
-        // mass check on the k = 0 mode (evolve.cu:145-155)
-        const double err = fabs(v[m].x * d.invN - d.scal[0]);
-        if (!(err <= d.comperr)) {
-          *d.stop_step = *d.base + s_local;
-          *d.status = kMassError;
-        }
+    }
+    if (t == 0 && j == 0 && kz == 0) {
+      // mass check on the k = 0 mode, held by slot m = 0 of thread 0 (evolve.cu:145-155)
+      const double err = fabs(v[0].x * d.invN - d.scal[0]);
+      if (!(err <= d.comperr)) {
+        *d.stop_step = *d.base + s_local;
+        *d.status = kMassError;
       }
     }
     store(d.Ch, v);
@@ -513,6 +529,30 @@ __global__ void __launch_bounds__(kBlock) k3_xspec(const Dev* __restrict__ dp, i
 }
 
 // ---- per-size kernel set ------------------------------------------------------------------
+// The plans of the coupled kernels are a type of their own.  Kernel and __device__
+// variable templates keyed on a plan (the pass-major twiddle table g_pass_tw<P, double>
+// and its fill kernel k_fill_pass_tw<P, double>) would otherwise be instantiated both
+// here and in the 2-D kernel units of the same size: such instances share one host
+// stub, so a launch from one unit could run (and fill the table of) the other unit's
+// module, leaving this unit's table unfilled.
+template <class Base>
+struct CphiPlan : Base {};
+// FP64 plans of at most 12 elements per thread: 128 and 256 take the eight-element
+// plans (4 4 8 and 4 8 8), whose transforms and twiddle powers fit two 256-thread
+// blocks per SM; the other sizes keep their FP64 plan (E <= 12 from 96 up).
+template <int N>
+struct CphiPlanOf {
+  using type = CphiPlan<typename Plan64<N>::type>;
+};
+template <>
+struct CphiPlanOf<128> {
+  using type = CphiPlan<Plan<128, 8, Radices<4, 4, 8>>>;
+};
+template <>
+struct CphiPlanOf<256> {
+  using type = CphiPlan<Plan<256, 8, Radices<4, 8, 8>>>;
+};
+
 struct Set {
   int n;
   size_t zsmem, lsmem;
@@ -529,7 +569,7 @@ struct Set {
 
 template <int N>
 struct SetOf {
-  using P = typename Plan64<N>::type;
+  using P = typename CphiPlanOf<N>::type;
   using ZG = ZGeom<P>;
   using LG = LGeom<P>;
   static void fill_tables(const void* tw, cudaStream_t st) {

@@ -142,6 +142,7 @@ _SIGNATURES = [
     ("esc_cphi_run_device", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, _vp, _i64p, ctypes.POINTER(ctypes.c_int)]),
     ("esc_cphi_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("esc_cphi_profile", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     ("esc_cphi_last_error", ctypes.c_char_p, [_vp]),
     ("esc_cphi_destroy", None, [_vp]),
 ]

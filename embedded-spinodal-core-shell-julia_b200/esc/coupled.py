@@ -113,6 +113,18 @@ class Coupled:
         self._check(st, done.value)
         return int(done.value), int(reason.value)
 
+    KERNELS = ("z fwd local", "y fwd x2", "x mu/phi", "y inv", "z inv mu + z stencil", "y stencil",
+               "x stencil", "z fwd div", "y fwd", "x c update", "y inv x2", "z inv final")
+
+    def profile(self, steps: int = 5):
+        """Mean time (ms) of each of the twelve kernels of a step (esc_cphi_profile),
+        stepping on from the fields of the last run."""
+        ms = np.zeros(12)
+        st = load_library().esc_cphi_profile(self._h, int(steps), _ptr(ms))
+        if st != ESC_OK:
+            raise EscError(st, self._err())
+        return dict(zip(self.KERNELS, ms.tolist()))
+
     def set_stream(self, stream_ptr: int) -> None:
         st = load_library().esc_cphi_set_stream(self._h, _vp(stream_ptr) if stream_ptr else None)
         if st != ESC_OK:

@@ -140,3 +140,20 @@ def test_coupled_rejects_bad_arguments():
     with pytest.raises(EscError):
         coupled.Coupled((16, 16, 16), spacing=(1.0, 0.0, 1.0))
     assert coupled.supported_axis(256) and not coupled.supported_axis(1024)
+
+
+def test_coupled_and_planar_runs_share_a_process():
+    """A 2-D run and a coupled run of the same grid size in one process, in both
+    orders: each keeps its own twiddle tables (the coupled kernel units must not
+    share kernel or table symbols with the 2-D units of the same size)."""
+    import esc
+    from esc import coupled
+    from oracle import core_shell_oracle as orc
+    c2, phi2 = orc.initial_fields(64, radius=16.0)
+    c3, phi3 = co.initial_fields(64, 64, 64, 18.0, seed=3)
+    ref2, _ = orc.run_simulation(c2, phi2, dt=0.01, steps=5)
+    ref3 = co.run(c3, phi3, co.CoupledParameters(), 0.01, 3)[0]
+    for _ in range(2):
+        a, _ = esc.run_simulation(c2, phi2, dt=0.01, steps=5)
+        b = coupled.run_coupled(c3, phi3, dt=0.01, steps=3)[0]
+        assert rel(a, ref2) < RTOL and rel(b, ref3) < RTOL
