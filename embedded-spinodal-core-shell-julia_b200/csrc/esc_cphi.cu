@@ -25,8 +25,10 @@ namespace cphi {
 constexpr int kFdW = 16;  // adjacent z lines per block of the stencil kernels
 
 // div += D_a(M D_a mu) along axis a = x (0) or y (1): each block stages kFdW
-// adjacent z lines of mu (n points each) in shared memory, forms q = M D mu,
-// then adds D q to div.  Runtime n; dynamic shared memory 2 n kFdW doubles.
+// adjacent z lines (n points each) of mu, of M = mobility h(phi) and of the
+// current div in shared memory -- every global load of the block is issued in
+// the first sweep --, turns the M tile into q = M D mu in place, then writes
+// div + D q.  Runtime n; dynamic shared memory 3 n kFdW doubles.
 __global__ void __launch_bounds__(kBlock) k3_fd_line(const Dev* __restrict__ dp, int axis) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const Dev& d = *dp;
@@ -39,8 +41,13 @@ __global__ void __launch_bounds__(kBlock) k3_fd_line(const Dev* __restrict__ dp,
   const long base = (long)blockIdx.y * ostride + k0;
   double* mt = reinterpret_cast<double*>(smraw);
   double* qt = mt + (size_t)n * kFdW;
+  double* dt = qt + (size_t)n * kFdW;
   const int total = n * kFdW;
   const double inv12 = 1.0 / (12.0 * h);
+  const double M0 = d.p.mobility;
+  const double* __restrict__ mu = d.mu;
+  const double* __restrict__ phi = d.phi;
+  double* __restrict__ div = d.div;
   // neighbour rows p +- 1, p +- 2 with the periodic wrap, without a runtime modulo
   auto row = [n](int p, int o) {
     int r = p + o;
@@ -50,39 +57,23 @@ __global__ void __launch_bounds__(kBlock) k3_fd_line(const Dev* __restrict__ dp,
   };
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int p = idx / kFdW, w = idx % kFdW;
-    mt[idx] = (k0 + w < d.nz) ? d.mu[base + (long)p * estride + w] : 0.0;
+    const bool ok = k0 + w < d.nz;
+    const long a = base + (long)p * estride + w;
+    mt[idx] = ok ? mu[a] : 0.0;
+    qt[idx] = ok ? mobility3(phi[a], M0) : 0.0;
+    dt[idx] = ok ? div[a] : 0.0;
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int p = idx / kFdW, w = idx % kFdW;
-    const double dm = fd4(mt[row(p, 2) + w], mt[row(p, 1) + w], mt[row(p, -1) + w], mt[row(p, -2) + w], inv12);
-    const double M = (k0 + w < d.nz) ? mobility3(d.phi[base + (long)p * estride + w], d.p.mobility) : 0.0;
-    qt[idx] = M * dm;
+    qt[idx] *= fd4(mt[row(p, 2) + w], mt[row(p, 1) + w], mt[row(p, -1) + w], mt[row(p, -2) + w], inv12);
   }
   __syncthreads();
-  // div += D q, four points per thread at a time: their div loads are issued
-  // together, ahead of the stores (which the compiler may not move loads across)
-  constexpr int U = 4;
-  for (int i0 = threadIdx.x; i0 < total; i0 += U * blockDim.x) {
-    double old[U];
-    long at[U];
-    bool ok[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int idx = i0 + u * blockDim.x;
-      const int p = idx / kFdW, w = idx % kFdW;
-      ok[u] = idx < total && k0 + w < d.nz;
-      at[u] = base + (long)p * estride + w;
-      old[u] = ok[u] ? d.div[at[u]] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (!ok[u]) continue;
-      const int idx = i0 + u * blockDim.x;
-      const int p = idx / kFdW, w = idx % kFdW;
-      const double dq = fd4(qt[row(p, 2) + w], qt[row(p, 1) + w], qt[row(p, -1) + w], qt[row(p, -2) + w], inv12);
-      d.div[at[u]] = old[u] + dq;
-    }
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int p = idx / kFdW, w = idx % kFdW;
+    if (k0 + w >= d.nz) continue;
+    div[base + (long)p * estride + w] =
+        dt[idx] + fd4(qt[row(p, 2) + w], qt[row(p, 1) + w], qt[row(p, -1) + w], qt[row(p, -2) + w], inv12);
   }
 }
 
@@ -268,9 +259,9 @@ void launch_step(esc_cphi& X, int s_local, cudaStream_t st, cudaEvent_t* ev = nu
   mark();
   X.sz->zi_mu(d, zb_pair, st);
   mark();
-  k3_fd_line<<<gfy, esc::kBlock, (size_t)2 * X.ny * kFdW * sizeof(double), st>>>(d, 1);
+  k3_fd_line<<<gfy, esc::kBlock, (size_t)3 * X.ny * kFdW * sizeof(double), st>>>(d, 1);
   mark();
-  k3_fd_line<<<gfx, esc::kBlock, (size_t)2 * X.nx * kFdW * sizeof(double), st>>>(d, 0);
+  k3_fd_line<<<gfx, esc::kBlock, (size_t)3 * X.nx * kFdW * sizeof(double), st>>>(d, 0);
   mark();
   X.sz->zf(d, kZDiv, zb_pair, st);
   mark();
@@ -458,7 +449,7 @@ esc_status esc_cphi_create(esc_cphi** out, int nx, int ny, int nz, double dx, do
     X.stream = X.own;
     for (const Set* s : {sx, sy, sz}) CK(s->prepare());
     CK(cudaFuncSetAttribute(k3_fd_line, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)(2 * 512 * kFdW * sizeof(double))));
+                            (int)(3 * 512 * kFdW * sizeof(double))));
     const size_t nn = (size_t)nx * ny * nz, nk = (size_t)nx * ny * X.K;
     Dev& h = X.h;
     h.nx = nx;

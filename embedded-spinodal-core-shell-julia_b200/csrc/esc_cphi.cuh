@@ -464,6 +464,14 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
 #pragma unroll
     for (int m = 0; m < E; ++m) arr[base + (long)(t + T * m) * estride] = make_double2(v[m].x, v[m].y);
   };
+  // L2 prefetch of the tile rows of an array read after a transform (one 128-byte
+  // line per 8 complex values of a row)
+  auto prefetch = [&](const double2* arr) {
+    if (active && (w & 7) == 0) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) prefetch_l2(arr + base + (long)(t + T * m) * estride);
+    }
+  };
   cpx<double> v[E];
   if (OP == kXInit) {
     load(d.D1, v);
@@ -475,6 +483,8 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
   } else if (OP == kXMu) {
     // mu^ = FFT(df/dc) + 2 kappa_c k^2 c^ (Compute_mu), back along x
     load(d.D1, v);
+    prefetch(d.Ch);
+    prefetch(d.Ph);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     const double kc2 = 2.0 * d.p.kappa_c;
 #pragma unroll
@@ -501,6 +511,7 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
   } else {
     // c^' = (dt div^ + lhs c^) / lhs, lhs = 1 + 2 Q kappa_c k^4 dt (kernel_comp_phi)
     load(d.D1, v);
+    prefetch(d.Ch);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     const double c1 = 2.0 * d.p.Q * d.p.kappa_c * d.dt;
 #pragma unroll
