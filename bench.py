@@ -22,6 +22,9 @@ is one time step of every particle (history row + stabilised update).
           drop-in per instance (max and L2 error of c, energy, mass drift), beside
           the FP64 drop-in restarted from c0 perturbed by 1e-8 relative, which
           measures how strongly the dynamics amplify any perturbation
+  coupled  the coupled c-phi model of the reference's 3-D program at its own input
+          (256^3, FP64): pt-steps/s, per-kernel times and HBM fractions, and the CPU
+          oracle on a 64^3 sample (--coupled-only runs this leg alone)
 
 The working set (1.7 GB mixed, 2.6 GB FP64) is far larger than the 126 MB L2,
 so no flush is needed between steps.  Under torchrun every rank runs its own
@@ -426,6 +429,9 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=2000)
     ap.add_argument("--no-large", action="store_true", help="skip the 1024^2 and 4096^2 single-grid runs")
     ap.add_argument("--no-coupled", action="store_true", help="skip the coupled c-phi 256^3 leg")
+    ap.add_argument("--gradients-only", action="store_true",
+                    help="run only the batched-gradient leg (64 x 512^2) and print its JSON object")
+    ap.add_argument("--gradient-steps", type=int, default=1000)
     ap.add_argument("--coupled-only", action="store_true",
                     help="run only the coupled c-phi 256^3 leg and print its JSON object")
     args = ap.parse_args()
@@ -445,6 +451,9 @@ def main():
     if args.coupled_only:
         print(json.dumps(coupled_block(read_peaks()[0], steps=args.steps, warmup=args.warmup,
                                        cpu=not args.no_cpu)), flush=True)
+        return 0
+    if args.gradients_only:
+        print(json.dumps(batched_gradient_block(steps=args.gradient_steps)), flush=True)
         return 0
     dist = None
     if world > 1:

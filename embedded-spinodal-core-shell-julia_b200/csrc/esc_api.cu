@@ -231,6 +231,11 @@ struct Engine {
     esc::InstDev* d_seed = nullptr;  // FP64 shadow instance with a 1-row history
     esc::InstDev* d_bwd = nullptr;   // FP64 shadow instance without history
     esc::InstDev* d_out = nullptr;   // final transform of the adjoint
+    // mixed contexts: the adjoint step transforms its derived fields in FP32
+    bool mixed = false;
+    esc::cpx2<float>* Gw = nullptr;  // FP32 pair array of the mixed step
+    esc::cpx<float>* Xw = nullptr;   // FP32 x-transform of g
+    esc::InstDev* d_bwd_m = nullptr; // mixed shadow instance for the forward row B kernel
     esc::AdjDev* d_adj = nullptr;    // one per step of a segment, per segment buffer
     double2* seg_buf[2] = {nullptr, nullptr};  // recomputed states of a segment (double-buffered)
     cudaStream_t sweep = nullptr;    // the adjoint sweep runs here, beside the next recompute
@@ -1125,7 +1130,8 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
     CK(A.ks64->prepare());
     CK(A.ks64->prepare_adj());
     if (A.ks64->warp_rows) CK(A.ks64->prepare_warp());
-    A.pstride = (size_t)A.ks64->part_len + 8 * 4096;
+    A.mixed = g.ks->wr_bytes == 4 && A.ks64->adj_col1_m != nullptr;
+    A.pstride = (size_t)std::max(A.ks64->part_len, g.ks->part_len) + 8 * 4096;
     TRY(E.alloc(&A.phi64, cnt * nn * 8, "adjoint phi"));
     TRY(E.alloc(&A.target, cnt * nn * 8, "adjoint target"));
     TRY(E.alloc(&A.cout, cnt * nn * 8, "adjoint output"));
@@ -1158,6 +1164,13 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
     }
     if (g.ks->sr_bytes == 8) CK(cudaMemcpy(A.tw64, g.tw_s, (size_t)n * 16, cudaMemcpyDeviceToDevice));
     A.ks64->fill_tables(A.tw64, A.tw64, st);
+    if (A.mixed) {
+      TRY(E.alloc(&A.Gw, cnt * hn * 16, "adjoint G (FP32)"));
+      TRY(E.alloc(&A.Xw, cnt * hn * 8, "adjoint Xg (FP32)"));
+      TRY(E.alloc(&A.d_bwd_m, cnt * sizeof(esc::InstDev), "adjoint descriptor"));
+      A.ks64->fill_adj32(g.tw_w, st);
+      if (g.ks->warp_rows) CK(g.ks->prepare_warp());
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     CK(cudaMemset(A.zero, 0, 4));
@@ -1218,7 +1231,7 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
   CK(cudaGetLastError());
   // ---- seed: energy, mu and lam_T at the final fields ----
   const esc::KernelSet* k64 = A.ks64;
-  std::vector<esc::InstDev> sd((size_t)cnt), bd((size_t)cnt), od((size_t)cnt);
+  std::vector<esc::InstDev> sd((size_t)cnt), bd((size_t)cnt), od((size_t)cnt), bm((size_t)cnt);
   std::vector<esc::AdjDev> ad((size_t)cnt);
   for (int s = 0; s < cnt; ++s) {
     esc::InstDev& q = sd[s];
@@ -1246,6 +1259,14 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
     od[s] = q;
     od[s].S = A.Lam + s * hn;
     od[s].hist = nullptr;
+    // the mixed forward row B kernel on the FP32 pair array and the FP32 particle field
+    bm[s] = bd[s];
+    if (A.mixed) {
+      bm[s].G = A.Gw + s * hn;
+      bm[s].phi = static_cast<const float*>(g.phi) + s * nn;
+      bm[s].tw_s = g.tw_s;
+      bm[s].tw_w = g.tw_w;
+    }
     esc::AdjDev& a = ad[s];
     memset(&a, 0, sizeof a);
     a.n = n;
@@ -1265,10 +1286,17 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
     a.part = A.part + s * A.pstride;
     a.cnt = A.acnt + 4 * s;
     a.acc = A.acc + 8 * s;
+    if (A.mixed) {
+      a.Gw = A.Gw + s * hn;
+      a.Xw = A.Xw + s * hn;
+      a.phiw = static_cast<const float*>(g.phi) + s * nn;
+    }
   }
   CK(cudaMemcpyAsync(A.d_seed, sd.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(A.d_bwd, bd.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(A.d_out, od.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
+  if (A.mixed)
+    CK(cudaMemcpyAsync(A.d_bwd_m, bm.data(), cnt * sizeof(esc::InstDev), cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(A.cnt, 0, cnt * 16, st));
   CK(cudaMemsetAsync(A.acnt, 0, cnt * 16, st));
   CK(cudaMemsetAsync(A.status, 0, cnt * 4, st));
@@ -1327,6 +1355,16 @@ esc_status engine_adjoint(Engine& E, const double* const* c0, int steps, double 
     esc::AdjDev* dd = A.d_adj + (size_t)b * K * cnt;
     TRY(adjoint_graph(E, 2, b, len, &gx, [&](cudaStream_t cs) {
       for (int j = len - 1; j >= 0; --j) {
+        if (A.mixed) {
+          k64->adj_col1_m(dd + (size_t)j * cnt, cnt, cs);
+          if (g.ks->warp_rows)
+            g.ks->row_b_w(A.d_bwd_m, cnt, A.zero, 0, cs);  // M grad a: the mixed forward row B
+          else
+            g.ks->row_b(A.d_bwd_m, cnt, A.zero, 0, cs);
+          k64->adj_col2_m(dd + (size_t)j * cnt, cnt, cs);
+          k64->adj_row2_m(dd + (size_t)j * cnt, cnt, cs);
+          continue;
+        }
         k64->adj_col1(dd + (size_t)j * cnt, cnt, cs);
         if (k64->warp_rows)
           k64->row_b_w(A.d_bwd, cnt, A.zero, 0, cs);  // M grad a: the forward row B, warp-independent form

@@ -111,10 +111,26 @@ __device__ __forceinline__ cpx<double> merge_half(const double2* __restrict__ a,
 // ---- z passes: lines along the contiguous axis, one group of T threads per unit --------
 enum ZMode { kZInit = 0, kZLocal = 1, kZDiv = 2 };
 
+// A line of at most 32 threads lives inside one warp: its exchanges use the
+// swizzled layout of the warp-independent 2-D row kernels and only __syncwarp;
+// larger groups use the padded row layout and block barriers.
 template <class P>
 struct ZGeom {
   static constexpr int N = P::N, E = P::E, T = P::T, G = kBlock / T, K = N / 2 + 1;
-  static constexpr size_t smem() { return (size_t)G * RowLayout<N>::stride * sizeof(cpx<double>); }
+  static constexpr bool kInWarp = T <= 32;
+  using Sync = typename std::conditional<kInWarp, WarpSync, BlockSync>::type;
+  using Lay = typename std::conditional<kInWarp, SwizzleLayout<N, sizeof(cpx<double>)>, RowLayout<N>>::type;
+  static constexpr size_t smem() {
+    return (size_t)G * (kInWarp ? N : RowLayout<N>::stride) * sizeof(cpx<double>);
+  }
+  // layout of group g of the block (its index inside the warp when lines share a warp)
+  static __device__ __forceinline__ Lay layout(int g) {
+    if constexpr (kInWarp) {
+      return Lay{g * N, (int)((threadIdx.x & 31) / T)};
+    } else {
+      return Lay{g * RowLayout<N>::stride};
+    }
+  }
 };
 
 // forward z transforms.  kZInit: (c + i phi) of line q -> D1 = c^, D2 = phi^;
@@ -161,11 +177,11 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zf(const Dev* __res
     v[m] = mkc<double>(a, b);
   }
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const RowLayout<N> lay{g * RowLayout<N>::stride};
-  fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
+  const auto lay = ZG::layout(g);
+  fft<false, P, typename ZG::Sync>(v, t, sm, lay, PassTable<P, double>{});
 #pragma unroll
   for (int m = 0; m < E; ++m) sm[lay(t + T * m)] = v[m];
-  __syncthreads();
+  ZG::Sync::sync();
   double2* oa = d.D1 + la * K;
   double2* ob = mode == kZDiv ? d.D1 + (la + 1) * K : d.D2 + la * K;
   if (active) {
@@ -199,8 +215,8 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_mu(const Dev* __
     v[m] = active ? merge_half<N>(d.D1 + la * K, hasb ? d.D1 + (la + 1) * K : nullptr, t + T * m)
                   : mkc<double>(0.0, 0.0);
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const RowLayout<N> lay{g * RowLayout<N>::stride};
-  fft<true, P>(v, t, sm, lay, PassTable<P, double>{});
+  const auto lay = ZG::layout(g);
+  fft<true, P, typename ZG::Sync>(v, t, sm, lay, PassTable<P, double>{});
   const double inv12 = 1.0 / (12.0 * d.dz);
 #pragma unroll
   for (int m = 0; m < E; ++m) {
@@ -212,7 +228,7 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_mu(const Dev* __
       if (hasb) d.mu[(la + 1) * N + x] = v[m].y;
     }
   }
-  __syncthreads();
+  ZG::Sync::sync();
   // q = M D_z mu at this thread's points (lane x: line a, lane y: line b)
   cpx<double> qv[E];
 #pragma unroll
@@ -228,10 +244,10 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_mu(const Dev* __
     }
     qv[m] = mkc<double>(Ma * dmx, Mb * dmy);
   }
-  __syncthreads();
+  ZG::Sync::sync();
 #pragma unroll
   for (int m = 0; m < E; ++m) sm[lay(t + T * m)] = qv[m];
-  __syncthreads();
+  ZG::Sync::sync();
   if (!active) return;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
@@ -335,8 +351,8 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_final(const Dev*
     co[m] = active ? cp[t + T * m] : 0.0;
   }
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
-  const RowLayout<N> lay{g * RowLayout<N>::stride};
-  fft<true, P>(v, t, sm, lay, PassTable<P, double>{});
+  const auto lay = ZG::layout(g);
+  fft<true, P, typename ZG::Sync>(v, t, sm, lay, PassTable<P, double>{});
   Six s = six_identity();
   if (active) {
     int nbad = 0;

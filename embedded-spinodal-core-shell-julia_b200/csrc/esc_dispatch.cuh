@@ -51,6 +51,12 @@ struct KernelSet {
   void (*adj_row2)(const AdjDev*, int, cudaStream_t);
   void (*adj_mu_col)(const AdjDev*, int, cudaStream_t);
   void (*adj_seed_row)(const AdjDev*, int, cudaStream_t);
+  // mixed-precision adjoint step kernels (FP64 kernel sets; for mixed contexts) and the
+  // fill of their FP32 pass-major twiddle tables from the plain FP32 table
+  void (*adj_col1_m)(const AdjDev*, int, cudaStream_t);
+  void (*adj_col2_m)(const AdjDev*, int, cudaStream_t);
+  void (*adj_row2_m)(const AdjDev*, int, cudaStream_t);
+  void (*fill_adj32)(const void*, cudaStream_t);
 };
 
 // Alternative column plans: fewer elements per thread (more passes, fewer
@@ -320,8 +326,23 @@ struct KS {
       if ((e = cudaFuncSetAttribute(k_adj_mu_col<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
       if ((e = cudaFuncSetAttribute(k_adj_seed_row<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)))
         return e;
+      if ((e = cudaFuncSetAttribute(k_adj_col1_m<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+      if ((e = cudaFuncSetAttribute(k_adj_col2_m<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+      if ((e = cudaFuncSetAttribute(k_adj_row2_m<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
     }
     return cudaSuccess;
+  }
+  static void adj_col1_m(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_col1_m<P><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(a);
+  }
+  static void adj_col2_m(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_col2_m<P><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(a);
+  }
+  static void adj_row2_m(const AdjDev* a, int count, cudaStream_t st) {
+    if constexpr (adj_ok) k_adj_row2_m<P><<<dim3(tiles_pairs, count), kBlock, smem(), st>>>(a);
+  }
+  static void fill_adj32(const void* tw32, cudaStream_t st) {
+    if constexpr (adj_ok) fill_one<P, float>(tw32, st);
   }
   static void adj_col1(const AdjDev* a, int count, cudaStream_t st) {
     if constexpr (adj_ok) k_adj_col1<P><<<dim3(tiles_cols, count), kBlock, smem(), st>>>(a);
@@ -396,6 +417,10 @@ struct KS {
     k.adj_col1 = adj_ok ? &adj_col1 : nullptr;
     k.adj_col2 = adj_ok ? &adj_col2 : nullptr;
     k.adj_row2 = adj_ok ? &adj_row2 : nullptr;
+    k.adj_col1_m = adj_ok ? &adj_col1_m : nullptr;
+    k.adj_col2_m = adj_ok ? &adj_col2_m : nullptr;
+    k.adj_row2_m = adj_ok ? &adj_row2_m : nullptr;
+    k.fill_adj32 = adj_ok ? &fill_adj32 : nullptr;
     k.adj_mu_col = adj_ok ? &adj_mu_col : nullptr;
     k.adj_seed_row = adj_ok ? &adj_seed_row : nullptr;
     return k;

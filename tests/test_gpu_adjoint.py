@@ -109,3 +109,31 @@ def test_batch_adjoint_rejects_mixed_sizes():
     with esc.Batch(phis, precision="fp64") as b:
         with pytest.raises(esc.EscError):
             b.adjoint(c0s, c0s, steps=3)
+
+
+@pytest.mark.parametrize("n,steps", [(256, 30), (512, 20)])
+def test_batch_adjoint_mixed_close_to_fp64(n, steps):
+    """Mixed contexts run the mixed adjoint step (FP64 adjoint state, FP32 derived-field
+    transforms): at the bench's grid sizes its batched gradients stay within the tolerances
+    of the single-particle mixed test of the FP64 gradients."""
+    lamF = 1e-3
+    base = orc.Parameters()
+    ps = [adj._with(base, P=base.P * f, chi=base.chi * g) for f, g in [(1.0, 1.0), (1.4, 0.8), (0.7, 1.3)]]
+    c0s, phis, cts = [], [], []
+    for i, p in enumerate(ps):
+        c0, phi = orc.initial_fields(n, radius=0.3 * n, width=2.0, seed=40 + i)
+        c0s.append(c0)
+        phis.append(phi)
+    with esc.Batch(phis, params=[_ep(adj._with(p, P=p.P * 1.1, chi=p.chi * 0.9)) for p in ps],
+                   precision="fp64") as bt:
+        cts, _, _ = bt.run(c0s, dt=0.01, steps=steps, with_history=False)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with esc.Batch(phis, params=[_ep(p) for p in ps], precision=prec) as b:
+            out[prec] = b.adjoint(c0s, cts, dt=0.01, steps=steps, lambda_F=lamF, ckpt_every=7)
+    L64, g64, th64 = out["fp64"]
+    L32, g32, th32 = out["mixed"]
+    for i in range(len(ps)):
+        assert abs(L32[i] - L64[i]) <= 1e-6 * abs(L64[i])
+        assert np.max(np.abs(g32[i] - g64[i])) <= 1e-4 * np.max(np.abs(g64[i]))
+        assert np.max(np.abs(np.asarray(th32[i]) - th64[i]) / np.abs(th64[i])) <= 1e-3, (i, th32[i], th64[i])
