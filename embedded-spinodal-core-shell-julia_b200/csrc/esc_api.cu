@@ -4,9 +4,9 @@
 // (run_simulation).  A context is a batch of one.  A batch groups its
 // instances by grid size; each group owns contiguous device buffers and a
 // device array of instance descriptors, and every phase kernel of a step is one
-// launch per group whose grid is (tiles, instances).  Steps are replayed from a
-// captured CUDA graph of kChunk steps; a device-side step counter gives each
-// launch its history row, so the graph never needs re-instantiation.
+// launch per group whose grid is (tiles, instances).  Steps are replayed from
+// captured CUDA graphs of 32, 16, 8, 4, 2 and 1 steps; a device-side step counter
+// gives each launch its history row, so the graphs never need re-instantiation.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -74,7 +74,6 @@ __global__ void k_fill_tuning_field(double* c, int n, int count) {
 __global__ void k_advance(int* base, int by) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *base += by;
 }
-constexpr int kChunk = 32;  // steps per captured graph
 // Graphs are captured for chunks of 32, 16, 8, 4, 2 and 1 steps, so that any step
 // count runs as at most K/32 + 5 graph launches per group.
 constexpr int kNumChunks = 6;
@@ -713,8 +712,8 @@ void launch_step(Engine& E, int s_local, cudaStream_t st) {
   }
 }
 
-// Each size group advances on its own stream: a captured graph of kChunk steps
-// of that group with its own step counter.  The groups' chains are independent
+// Each size group advances on its own stream: captured graphs of 32, 16, ..., 1
+// steps of that group with its own step counter.  The groups' chains are independent
 // (one instance never reads another), so they overlap on the GPU and fill each
 // other's launch tails, and in a run with host buffers one group's copies
 // overlap the other groups' steps.
