@@ -11,6 +11,12 @@ representation that reads back to the same double, in the style Julia prints
 Float64 (``0.5``, ``1.0e-5``, ``1.0e6``); Julia is not available to byte-compare
 the text, so the guarantee is numerical: every value reads back exactly.
 
+The coupled 3-D model writes configuration files in the layout of the reference's
+3-D program (original/2023-3d/out_conf.cu:39-43): ``conf.%09d`` named by the step,
+holding c and then phi as raw float64 in the order a[k + nz*(j + ny*i)] (z
+contiguous), with no header; the grid shape travels separately
+(`write_conf3d` / `read_conf3d`).
+
 The restart format is a raw little-endian binary file: a 64-byte header
 (magic ``ESCRST01``, int32 n, int32 flags, int64 step, float64 dt, float64 dx,
 float64 time, 16 reserved bytes) followed by c (n*n float64, the bytes of the
@@ -139,3 +145,33 @@ def load_restart(path: str) -> Tuple[np.ndarray, Optional[np.ndarray], dict]:
     c = np.frombuffer(body[: n * n * 8], dtype="<f8").reshape(n, n).copy()
     phi = np.frombuffer(body[n * n * 8:], dtype="<f8").reshape(n, n).copy() if flags & 1 else None
     return c, phi, {"step": int(step), "dt": float(dt), "dx": float(dx), "time": float(t)}
+
+
+def conf3d_name(step: int) -> str:
+    """File name of a 3-D configuration after `step` steps: ``conf.%09d`` (out_conf.cu:39)."""
+    return "conf.%09d" % int(step)
+
+
+def write_conf3d(directory: str, step: int, c: np.ndarray, phi: np.ndarray) -> str:
+    """Writes c then phi (float64, C order of shape (nx, ny, nz), i.e. z contiguous) to
+    ``directory/conf.%09d`` like the reference's Output_conf (out_conf.cu:39-43); returns the path."""
+    c = np.ascontiguousarray(c, dtype="<f8")
+    phi = np.ascontiguousarray(phi, dtype="<f8")
+    if c.shape != phi.shape or c.ndim != 3:
+        raise ValueError("c and phi must be 3-D arrays of one shape")
+    os.makedirs(directory, exist_ok=True)
+    path = os.path.join(directory, conf3d_name(step))
+    with open(path, "wb") as f:
+        f.write(c.tobytes())
+        f.write(phi.tobytes())
+    return path
+
+
+def read_conf3d(path: str, shape: Tuple[int, int, int]) -> Tuple[np.ndarray, np.ndarray]:
+    """Reads a configuration file of `write_conf3d` (or of the reference's 3-D program)
+    for a grid of `shape` = (nx, ny, nz); returns (c, phi)."""
+    n = int(np.prod(shape))
+    raw = np.fromfile(path, dtype="<f8")
+    if raw.size != 2 * n:
+        raise ValueError(f"{path}: {raw.size} values, expected {2 * n} for shape {tuple(shape)}")
+    return raw[:n].reshape(shape).copy(), raw[n:].reshape(shape).copy()

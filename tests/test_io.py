@@ -65,3 +65,18 @@ def test_restart_rejects_bad_files(tmp_path):
     good.write_bytes(good.read_bytes()[:-8])
     with pytest.raises(ValueError):
         io.load_restart(str(good))
+
+
+def test_conf3d_round_trip(tmp_path):
+    """3-D configuration files: c then phi, raw float64, z contiguous (out_conf.cu:39-43)."""
+    rng = np.random.default_rng(3)
+    c, phi = rng.random((4, 6, 8)), rng.random((4, 6, 8))
+    path = io.write_conf3d(str(tmp_path), 120, c, phi)
+    assert os.path.basename(path) == "conf.000000120"
+    assert os.path.getsize(path) == 2 * c.size * 8
+    raw = np.fromfile(path, dtype="<f8")
+    assert raw[1] == c[0, 0, 1] and raw[8] == c[0, 1, 0] and raw[c.size] == phi[0, 0, 0]
+    c2, phi2 = io.read_conf3d(path, c.shape)
+    assert np.array_equal(c2, c) and np.array_equal(phi2, phi)
+    with pytest.raises(ValueError):
+        io.read_conf3d(path, (4, 6, 7))
