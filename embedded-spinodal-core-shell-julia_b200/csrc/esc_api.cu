@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "esc.h"
+#include "esc_cluster.h"
 #include "esc_dispatch.cuh"
 
 #define ESC_DECL(n) const esc::KernelSet* esc_kernels_##n(int prec);
@@ -212,6 +213,9 @@ struct Engine {
   int* h_status = nullptr;
   long long* h_bad = nullptr;
   bool pending = false;  // a device-memory run was queued and not yet waited for
+  // a single FP64 grid of a size with a cluster configuration runs its whole loop
+  // in one cluster launch (esc_cluster.cu) instead of four launches per step
+  bool cluster = false;
   std::vector<void*> allocs;
   std::string err;
   // adjoint resources (allocated on first use; single-instance contexts)
@@ -790,6 +794,54 @@ esc_status launch_steps(Engine& E, Group& g, int steps, cudaStream_t ss) {
   return ESC_OK;
 }
 
+// ESC_CLUSTER=0 keeps single grids on the launch-per-phase path
+bool cluster_knob() {
+  const char* v = getenv("ESC_CLUSTER");
+  return !(v && v[0] == '0');
+}
+
+// Single FP64 contexts of n = 128 or 256 run in one cluster launch when the
+// device can place the cluster: its twiddle tables are filled here, and the
+// status words of queued runs come back through the pinned host slots.
+esc_status enable_cluster(Engine& E) {
+  if (E.count != 1 || E.prec != ESC_FP64 || E.groups.size() != 1 || !cluster_knob()) return ESC_OK;
+  Group& g = E.groups[0];
+  if (g.ks->generic || !esc::clu::available(g.n)) return ESC_OK;
+  DeviceGuard dg(E.device);
+  CK(esc::clu::prepare(g.n, g.tw_s, E.own));
+  if (!E.h_status) {
+    CK(cudaMallocHost(reinterpret_cast<void**>(&E.h_status), sizeof(int)));
+    CK(cudaMallocHost(reinterpret_cast<void**>(&E.h_bad), sizeof(long long)));
+  }
+  CK(cudaStreamSynchronize(E.own));
+  E.cluster = true;
+  return ESC_OK;
+}
+
+// Queues a cluster run of the single grid on the engine's stream: status words,
+// the launch, and the status copies into the pinned host slots.
+esc_status cluster_enqueue(Engine& E, double* cdev, int steps, double dt, double* hist) {
+  Group& g = E.groups[0];
+  cudaStream_t st = E.stream;
+  CK(cudaMemsetAsync(g.status, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(g.bad, 0xff, sizeof(long long), st));
+  esc::clu::Args a;
+  a.phi = static_cast<const double*>(g.phi);
+  a.c = cdev;
+  a.hist = hist;
+  a.hist_ld = steps + 1;
+  a.steps = steps;
+  a.dt = dt;
+  a.dx = g.h_inst[0].dx;
+  a.p = g.h_inst[0].p;
+  a.status = g.status;
+  a.bad_step = g.bad;
+  CK(esc::clu::run(g.n, a, st));
+  CK(cudaMemcpyAsync(E.h_status, g.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(E.h_bad, g.bad, sizeof(long long), cudaMemcpyDeviceToHost, st));
+  return ESC_OK;
+}
+
 // c_in_out: per-instance pointers (host or device per `device_io`);
 // hist_host: per-instance host pointers (entries may be null) or null;
 // hist_dev: one device array for all instances or null.
@@ -824,6 +876,22 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
     hbase = E.hist;
   }
   cudaStream_t st = E.stream;
+  if (E.cluster) {
+    Group& g = E.groups[0];
+    const size_t nn = (size_t)g.n * g.n;
+    double* cdev = device_io ? cptr[0] : g.cio;
+    if (!device_io) CK(cudaMemcpyAsync(g.cio, cptr[0], nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    TRY(cluster_enqueue(E, cdev, steps, dt, hbase));
+    CK(cudaStreamSynchronize(st));
+    const int status = *E.h_status;
+    const long long bad = *E.h_bad;
+    if (!device_io && status == 0) CK(cudaMemcpy(cptr[0], g.cio, nn * sizeof(double), cudaMemcpyDeviceToHost));
+    if (hist_host && hist_host[0]) CK(cudaMemcpy(hist_host[0], hbase, per * sizeof(double), cudaMemcpyDeviceToHost));
+    if (bad_out) bad_out[0] = status ? (int64_t)bad : -1;
+    (void)leave_bad_unchanged;
+    if (status) return E.fail(ESC_ENONFINITE, "Non-finite composition at step " + std::to_string(bad));
+    return ESC_OK;
+  }
   for (Group& g : E.groups) {
     const size_t nn = (size_t)g.n * g.n;
     for (size_t s = 0; s < g.members.size(); ++s) {
@@ -978,6 +1046,11 @@ esc_status engine_enqueue_device(Engine& E, double* const* cptr, int steps, doub
     hbase = E.hist;
   }
   cudaStream_t st = E.stream;
+  if (E.cluster) {
+    TRY(cluster_enqueue(E, cptr[0], steps, dt, hbase));
+    E.pending = true;
+    return ESC_OK;
+  }
   TRY(ensure_graph(E));
   for (Group& g : E.groups) {
     for (size_t s = 0; s < g.members.size(); ++s) {
@@ -1456,6 +1529,7 @@ esc_status esc_create(esc_ctx** out, int n, double dx, const double* phi, const 
     std::lock_guard<std::mutex> lock(creation_mutex());
     s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
     if (s == ESC_OK) s = autotune(c->e);
+    if (s == ESC_OK) s = enable_cluster(c->e);
     if (s == ESC_OK) s = ensure_graph(c->e);
   }
   if (s != ESC_OK) {
@@ -1512,6 +1586,8 @@ esc_status esc_wait(esc_ctx* ctx, int64_t* bad_step) {
   if (bad_step) *bad_step = b;
   return s;
 }
+
+int esc_uses_cluster(const esc_ctx* ctx) { return ctx && ctx->e.cluster ? 1 : 0; }
 
 esc_status esc_set_stream(esc_ctx* ctx, void* stream) {
   if (!ctx) return ESC_EINVAL;

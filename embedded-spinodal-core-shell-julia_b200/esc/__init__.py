@@ -106,6 +106,7 @@ _SIGNATURES = [
     ("esc_run_device_async", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, _vp]),
     ("esc_wait", ctypes.c_int, [_vp, _i64p]),
     ("esc_last_error", ctypes.c_char_p, [_vp]),
+    ("esc_uses_cluster", ctypes.c_int, [_vp]),
     ("esc_destroy", None, [_vp]),
     ("esc_adjoint", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_int,
                                    _dp, _dp, _dp]),
@@ -288,6 +289,11 @@ class Context:
         st = load_library().esc_wait(self._h, ctypes.byref(bad))
         if st != ESC_OK:
             _raise(st, self._err(), bad.value)
+
+    @property
+    def uses_cluster(self) -> bool:
+        """True when this context's runs go through the cluster-resident kernel (esc_uses_cluster)."""
+        return bool(load_library().esc_uses_cluster(self._h))
 
     def set_stream(self, stream_ptr: int) -> None:
         st = load_library().esc_set_stream(self._h, _vp(stream_ptr) if stream_ptr else None)
