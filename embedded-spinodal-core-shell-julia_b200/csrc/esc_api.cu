@@ -794,10 +794,15 @@ esc_status launch_steps(Engine& E, Group& g, int steps, cudaStream_t ss) {
   return ESC_OK;
 }
 
-// ESC_CLUSTER=0 keeps single grids on the launch-per-phase path
+// ESC_CLUSTER=0 keeps single grids on the launch-per-phase path, ESC_CLUSTER=1
+// takes the cluster path without timing it; unset, the faster of the two is kept
 bool cluster_knob() {
   const char* v = getenv("ESC_CLUSTER");
   return !(v && v[0] == '0');
+}
+bool cluster_forced() {
+  const char* v = getenv("ESC_CLUSTER");
+  return v && v[0] == '1';
 }
 
 // Single FP64 contexts of n = 128 or 256 run in one cluster launch when the
@@ -1125,6 +1130,48 @@ esc_status engine_wait(Engine& E, int64_t* bad_out) {
         return E.fail(ESC_ENONFINITE, "Non-finite composition at step " + std::to_string(bad[i]) +
                                           (E.count > 1 ? " (instance " + std::to_string(i) + ")" : ""));
   }
+  return ESC_OK;
+}
+
+// Times 16 steps of the cluster path and of the launch-per-phase path on a smooth
+// synthetic field and keeps the faster for this context (the decision is cached
+// per grid size and device; creations are serialised).
+esc_status choose_cluster(Engine& E) {
+  if (!E.cluster || cluster_forced()) return ESC_OK;
+  static std::map<std::pair<int, int>, bool> decided;
+  Group& g = E.groups[0];
+  const auto key = std::make_pair(g.n, E.device);
+  auto it = decided.find(key);
+  if (it != decided.end()) {
+    E.cluster = it->second;
+    return ESC_OK;
+  }
+  DeviceGuard dg(E.device);
+  cudaStream_t st = E.stream;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto time_path = [&](bool cluster, float* ms) -> esc_status {
+    E.cluster = cluster;
+    double* cp[1] = {g.cio};
+    for (int rep = 0; rep < 2; ++rep) {  // the first run builds and uploads what the path needs
+      k_fill_tuning_field<<<1024, 256, 0, st>>>(g.cio, g.n, 1);
+      CK(cudaEventRecord(e0, st));
+      TRY(engine_enqueue_device(E, cp, 16, 0.01, nullptr));
+      CK(cudaEventRecord(e1, st));
+      TRY(engine_wait(E, nullptr));
+    }
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    return ESC_OK;
+  };
+  float t_cluster = 0.f, t_phases = 0.f;
+  esc_status rs = time_path(true, &t_cluster);
+  if (rs == ESC_OK) rs = time_path(false, &t_phases);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rs != ESC_OK) return rs;
+  E.cluster = t_cluster < t_phases;
+  decided[key] = E.cluster;
   return ESC_OK;
 }
 
@@ -1530,6 +1577,7 @@ esc_status esc_create(esc_ctx** out, int n, double dx, const double* phi, const 
     s = engine_create(c->e, 1, &n, &dx, phis, p, (int)prec);
     if (s == ESC_OK) s = autotune(c->e);
     if (s == ESC_OK) s = enable_cluster(c->e);
+    if (s == ESC_OK) s = choose_cluster(c->e);
     if (s == ESC_OK) s = ensure_graph(c->e);
   }
   if (s != ESC_OK) {

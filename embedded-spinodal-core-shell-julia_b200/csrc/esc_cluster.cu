@@ -39,30 +39,34 @@ namespace clu {
 template <class Base>
 struct CPlan : Base {};
 
-constexpr int kThreads = 256;
-
-template <int N, int C>
-struct Geo {
-  static constexpr int H = N / 2, R = N / C, NP = R / 2, NC = H / C;
-  static constexpr int TA = kThreads / NP, TB = kThreads / R, TC = kThreads / NC;
-};
-template <int N, int C>
-struct Plans;
+// Configuration per grid size: cluster size C and threads per CTA
+template <int N>
+struct Config;
 template <>
-struct Plans<256, 16> {  // row pairs and columns: 32 threads, 8 elements; rows: 16 threads, 16 elements
+struct Config<256> {  // 16 CTAs of 256 threads: row pairs and columns 32 threads x 8 elements, rows 16 x 16
+  // (512 threads with 4- and 8-element plans measured slower: 42.1 against 36.4 us per step)
+  static constexpr int C = 16, TH = 256;
   using A = CPlan<Plan<256, 8, Radices<8, 8, 4>>>;
   using B = CPlan<Plan<256, 16, Radices<16, 16>>>;
 };
 template <>
-struct Plans<128, 8> {   // row pairs and columns: 32 threads, 4 elements; rows: 16 threads, 8 elements
+struct Config<128> {  // 8 CTAs of 256 threads: row pairs and columns 32 x 4, rows 16 x 8
+  static constexpr int C = 8, TH = 256;
   using A = CPlan<Plan<128, 4, Radices<4, 4, 4, 2>>>;
   using B = CPlan<Plan<128, 8, Radices<8, 8, 2>>>;
 };
 
+template <int N>
+struct Geo {
+  static constexpr int C = Config<N>::C, TH = Config<N>::TH;
+  static constexpr int H = N / 2, R = N / C, NP = R / 2, NC = H / C, NW = TH / 32;
+  static constexpr int TA = TH / NP, TB = TH / R, TC = TH / NC;
+};
+
 // shared-memory layout of one CTA
-template <int N, int C>
+template <int N>
 struct Smem {
-  using G_ = Geo<N, C>;
+  using G_ = Geo<N>;
   static constexpr int H = G_::H, R = G_::R;
   static constexpr size_t s_elems = (size_t)R * H;                       // cpx<double>
   static constexpr size_t g_elems = (size_t)R * H;                       // cpx2<double>
@@ -77,27 +81,28 @@ struct Smem {
   static constexpr size_t bytes = off_part + part_doubles * 8;
 };
 
-// deterministic block sum (fixed order) of NV values; result valid in thread 0
-template <int NV>
-__device__ __forceinline__ void block_sums(double (&v)[NV], double* red /* 8 * NV */) {
+// deterministic block sum (fixed order) of NV values over NW warps; result valid in thread 0
+template <int NW, int NV>
+__device__ __forceinline__ void block_sums(double (&v)[NV], double* red /* NW * NV */) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
   if (lane == 0) {
 #pragma unroll
-    for (int q = 0; q < NV; ++q) red[q * 8 + wid] = v[q];
+    for (int q = 0; q < NV; ++q) red[q * NW + wid] = v[q];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       double s = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) s += red[q * 8 + w];
+      for (int w = 0; w < NW; ++w) s += red[q * NW + w];
       v[q] = s;
     }
   }
   __syncthreads();
 }
+template <int NW>
 __device__ __forceinline__ double block_minmax(double v, double* red, bool is_max) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   v = is_max ? warp_max(v) : warp_min(v);
@@ -105,7 +110,7 @@ __device__ __forceinline__ double block_minmax(double v, double* red, bool is_ma
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = red[0];
-    for (int w = 1; w < kThreads / 32; ++w) s = is_max ? fmax(s, red[w]) : fmin(s, red[w]);
+    for (int w = 1; w < NW; ++w) s = is_max ? fmax(s, red[w]) : fmin(s, red[w]);
     v = s;
   }
   __syncthreads();
@@ -126,18 +131,19 @@ __device__ __forceinline__ cpx<double> pair_spectrum_sm(const cpx<double>* a, co
 }
 
 // The persistent cluster kernel: c -> S, then steps s = 0..steps (history row s;
-// the update only for s < steps), then S -> c.  One cluster, kThreads threads per CTA.
-template <int N, int C>
-__global__ void __launch_bounds__(kThreads, 1) k_cluster_run(const Args a) {
-  using G_ = Geo<N, C>;
-  using SM = Smem<N, C>;
-  using PA = typename Plans<N, C>::A;
-  using PB = typename Plans<N, C>::B;
+// the update only for s < steps), then S -> c.  One cluster of Config<N>::C CTAs.
+template <int N>
+__global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) {
+  using G_ = Geo<N>;
+  using SM = Smem<N>;
+  using PA = typename Config<N>::A;
+  using PB = typename Config<N>::B;
+  constexpr int C = G_::C, NW = G_::NW;
   constexpr int H = G_::H, R = G_::R, NC = G_::NC;
   constexpr int EA = PA::E, TA = PA::T, EB = PB::E, TB = PB::T;
   static_assert(TA == G_::TA && TB == G_::TB && TA == G_::TC, "plan geometry");
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double red[8 * 8];
+  __shared__ double red[6 * NW];
   __shared__ double fold[8];
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
@@ -206,9 +212,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_cluster_run(const Args a) {
         Gs[(size_t)(la + 1) * H + t + TA * m].a = xb[m];
       }
       double sums[3] = {sc, sf, bad};
-      block_sums<3>(sums, red);
-      const double bmn = block_minmax(mn, red + 32, false);
-      const double bmx = block_minmax(mx, red + 40, true);
+      block_sums<NW, 3>(sums, red);
+      const double bmn = block_minmax<NW>(mn, red + 3 * NW, false);
+      const double bmx = block_minmax<NW>(mx, red + 4 * NW, true);
       if (threadIdx.x == 0) {
         part[0] = sums[0];
         part[1] = bmn;
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_cluster_run(const Args a) {
         dst[(size_t)(y % R) * H + kx] = o;
       }
       double e1[1] = {gsum};
-      block_sums<1>(e1, red);
+      block_sums<NW, 1>(e1, red);
       if (threadIdx.x == 0) part[5] = e1[0];
     }
     cl.sync();
@@ -385,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_cluster_run(const Args a) {
         row[t + TB * m] = o;
       }
       double d1[1] = {dsum};
-      block_sums<1>(d1, red);
+      block_sums<NW, 1>(d1, red);
       if (threadIdx.x == 0) part[6] = d1[0];
     }
     cl.sync();
@@ -461,7 +467,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_cluster_run(const Args a) {
 #pragma unroll
         for (int m = 0; m < EA; ++m) colsum[0] += fa[m].x;
       }
-      block_sums<1>(colsum, red);
+      block_sums<NW, 1>(colsum, red);
       if (threadIdx.x == 0) fold[5] = colsum[0];
       __syncthreads();
       const double corr = packed ? fold[5] / (double)N : 0.0;
@@ -497,15 +503,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_cluster_run(const Args a) {
 }
 
 // ---- host side -----------------------------------------------------------------------
-template <int N, int C>
+template <int N>
 struct Launcher {
-  using PA = typename Plans<N, C>::A;
-  using PB = typename Plans<N, C>::B;
-  static constexpr size_t kSmem = Smem<N, C>::bytes;
+  using PA = typename Config<N>::A;
+  using PB = typename Config<N>::B;
+  static constexpr int C = Config<N>::C, TH = Config<N>::TH;
+  static constexpr size_t kSmem = Smem<N>::bytes;
   static cudaLaunchConfig_t config(cudaStream_t st, cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);
-    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.blockDim = dim3(TH, 1, 1);
     cfg.dynamicSmemBytes = kSmem;
     cfg.stream = st;
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -518,9 +525,9 @@ struct Launcher {
   }
   static cudaError_t attributes() {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_cluster_run<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)))
+    if ((e = cudaFuncSetAttribute(k_cluster_run<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)))
       return e;
-    if (C > 8 && (e = cudaFuncSetAttribute(k_cluster_run<N, C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)))
+    if (C > 8 && (e = cudaFuncSetAttribute(k_cluster_run<N>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)))
       return e;
     return cudaSuccess;
   }
@@ -532,7 +539,7 @@ struct Launcher {
     cudaLaunchAttribute attr[1];
     const cudaLaunchConfig_t cfg = config(nullptr, attr);
     int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, k_cluster_run<N, C>, &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_cluster_run<N>, &cfg) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
@@ -548,7 +555,7 @@ struct Launcher {
   static cudaError_t run(const Args& a, cudaStream_t st) {
     cudaLaunchAttribute attr[1];
     const cudaLaunchConfig_t cfg = config(st, attr);
-    return cudaLaunchKernelEx(&cfg, k_cluster_run<N, C>, a);
+    return cudaLaunchKernelEx(&cfg, k_cluster_run<N>, a);
   }
 };
 
@@ -568,19 +575,19 @@ bool available(int n) {
   const int si = n == 256 ? 0 : (n == 128 ? 1 : -1);
   if (si < 0) return false;
   std::lock_guard<std::mutex> lock(avail_mutex());
-  if (!cache[dev][si]) cache[dev][si] = (si == 0 ? Launcher<256, 16>::available() : Launcher<128, 8>::available()) ? 1 : -1;
+  if (!cache[dev][si]) cache[dev][si] = (si == 0 ? Launcher<256>::available() : Launcher<128>::available()) ? 1 : -1;
   return cache[dev][si] > 0;
 }
 
 cudaError_t prepare(int n, const void* tw, cudaStream_t st) {
-  if (n == 256) return Launcher<256, 16>::prepare(tw, st);
-  if (n == 128) return Launcher<128, 8>::prepare(tw, st);
+  if (n == 256) return Launcher<256>::prepare(tw, st);
+  if (n == 128) return Launcher<128>::prepare(tw, st);
   return cudaErrorInvalidValue;
 }
 
 cudaError_t run(int n, const Args& a, cudaStream_t st) {
-  if (n == 256) return Launcher<256, 16>::run(a, st);
-  if (n == 128) return Launcher<128, 8>::run(a, st);
+  if (n == 256) return Launcher<256>::run(a, st);
+  if (n == 128) return Launcher<128>::run(a, st);
   return cudaErrorInvalidValue;
 }
 

@@ -1,9 +1,11 @@
 """Cluster-resident runs of single small FP64 grids (csrc/esc_cluster.cu).
 
-A single 128^2 or 256^2 FP64 context runs its whole time loop in one launch of
-one thread-block cluster, the state in distributed shared memory.  These tests
-hold that path to the CPU oracle (core_shell.jl:84-103 restated) at 1e-12, to the
-launch-per-phase path (ESC_CLUSTER=0) at the rounding level, and check its
+A single 128^2 or 256^2 FP64 context can run its whole time loop in one launch
+of one thread-block cluster, the state in distributed shared memory; at creation
+the library times that path against the launch-per-phase path and keeps the
+faster (ESC_CLUSTER=1 forces the cluster path, 0 forbids it).  These tests force
+the cluster path and hold it to the CPU oracle (core_shell.jl:84-103 restated) at
+1e-12 and to the launch-per-phase path at the rounding level, and check its
 non-finite stop, its queued device-memory entry points and its history."""
 import numpy as np
 import pytest
@@ -12,6 +14,11 @@ import esc
 from oracle import core_shell_oracle as orc
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _force_cluster(monkeypatch):
+    monkeypatch.setenv("ESC_CLUSTER", "1")
 
 RTOL = 1e-12
 
@@ -80,3 +87,15 @@ def test_cluster_path_queued_device_run():
         ctx.wait()
         assert np.array_equal(d.cpu().numpy(), c)
         assert np.array_equal(dh.cpu().numpy().reshape(6, 34).T, h)
+
+
+@pytest.mark.parametrize("n", [128, 256])
+def test_timed_choice_gives_oracle_results(n, monkeypatch):
+    """Unforced, the creation times both paths and keeps the faster; either way the
+    results are the oracle's."""
+    monkeypatch.delenv("ESC_CLUSTER", raising=False)
+    c0, phi = orc.initial_fields(n, radius=0.3 * n, width=2.0, seed=23)
+    with esc.Context(phi) as ctx:
+        c, h = ctx.run(c0, dt=0.01, steps=12)
+    co, ho = orc.run_simulation(c0, phi, dt=0.01, steps=12)
+    assert rel(c, co) < RTOL and hist_rel(h, ho) < RTOL
