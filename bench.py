@@ -432,6 +432,8 @@ def main():
     ap.add_argument("--gradients-only", action="store_true",
                     help="run only the batched-gradient leg (64 x 512^2) and print its JSON object")
     ap.add_argument("--gradient-steps", type=int, default=1000)
+    ap.add_argument("--default-example-only", action="store_true",
+                    help="run only the 256^2 default example of core_shell.jl (1000 steps, FP64 and mixed)")
     ap.add_argument("--coupled-only", action="store_true",
                     help="run only the coupled c-phi 256^3 leg and print its JSON object")
     args = ap.parse_args()
@@ -451,6 +453,13 @@ def main():
     if args.coupled_only:
         print(json.dumps(coupled_block(read_peaks()[0], steps=args.steps, warmup=args.warmup,
                                        cpu=not args.no_cpu)), flush=True)
+        return 0
+    if args.default_example_only:
+        from esc import fields
+        phi0 = fields.particle_disc(256, radius=70.0, width=4.0)
+        c00 = fields.interior_noise(phi0, 5749)
+        print(json.dumps(single_grid_block("256^2 default example (disc R=70, w=4), 1000 steps", phi0, c00, 1000,
+                                           read_peaks()[0])), flush=True)
         return 0
     if args.gradients_only:
         print(json.dumps(batched_gradient_block(steps=args.gradient_steps)), flush=True)
