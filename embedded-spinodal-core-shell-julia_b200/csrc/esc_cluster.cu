@@ -70,14 +70,14 @@ struct Smem {
   static constexpr int H = G_::H, R = G_::R;
   static constexpr size_t s_elems = (size_t)R * H;                       // cpx<double>
   static constexpr size_t g_elems = (size_t)R * H;                       // cpx2<double>
-  static constexpr size_t xa = (size_t)G_::NP * RowLayout<N>::stride;   // row A / init / final exchange
-  static constexpr size_t xb = (size_t)R * RowLayout<N>::stride;         // row B exchange
+  static constexpr size_t xa = (size_t)G_::NP * N;   // row A / init / final exchange (one swizzled line per group)
+  static constexpr size_t xb = (size_t)R * N;          // row B exchange
   static constexpr size_t xc = (size_t)((N * G_::NC - 1) + ((N * G_::NC - 1) >> 4)) + 1;  // column exchange
   static constexpr size_t x_elems = xa > xb ? (xa > xc ? xa : xc) : (xb > xc ? xb : xc);
   static constexpr size_t off_g = s_elems * 16;
   static constexpr size_t off_x = off_g + g_elems * 32;
   static constexpr size_t off_part = off_x + x_elems * 16;
-  static constexpr size_t part_doubles = 16;  // [0..4] row A, [5] energy, [6] dissipation
+  static constexpr size_t part_doubles = 7 * G_::NW;  // per warp: row A's five sums, energy, dissipation
   static constexpr size_t bytes = off_part + part_doubles * 8;
 };
 
@@ -102,21 +102,6 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* red /* NW * 
   }
   __syncthreads();
 }
-template <int NW>
-__device__ __forceinline__ double block_minmax(double v, double* red, bool is_max) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  v = is_max ? warp_max(v) : warp_min(v);
-  if (lane == 0) red[wid] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = red[0];
-    for (int w = 1; w < NW; ++w) s = is_max ? fmax(s, red[w]) : fmin(s, red[w]);
-    v = s;
-  }
-  __syncthreads();
-  return v;
-}
-
 // full spectrum of two real rows a, b from their packed half spectra in shared memory
 template <int N>
 __device__ __forceinline__ cpx<double> pair_spectrum_sm(const cpx<double>* a, const cpx<double>* b, int k) {
@@ -142,6 +127,7 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
   constexpr int H = G_::H, R = G_::R, NC = G_::NC;
   constexpr int EA = PA::E, TA = PA::T, EB = PB::E, TB = PB::T;
   static_assert(TA == G_::TA && TB == G_::TB && TA == G_::TC, "plan geometry");
+  static_assert(TA <= 32 && 32 % TA == 0 && TB <= 32 && 32 % TB == 0, "row groups inside one warp");
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[6 * NW];
   __shared__ double fold[8];
@@ -158,7 +144,7 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
   // ---- c -> S: row pairs of this CTA (forward x-transform, split) ----
   {
     const int t = threadIdx.x % TA, pr = threadIdx.x / TA;
-    const RowLayout<N> lay{pr * RowLayout<N>::stride};
+    const SwizzleLayout<N, sizeof(cpx<double>)> lay{pr * N, (int)((threadIdx.x & 31) / TA)};
     const int ya = y0 + 2 * pr;
     cpx<double> v[EA];
 #pragma unroll
@@ -166,9 +152,9 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
       const int x = t + TA * m;
       v[m] = mkc<double>(a.c[(size_t)ya * N + x], a.c[(size_t)(ya + 1) * N + x]);
     }
-    fft<false, PA>(v, t, X, lay, PassTable<PA, double>{});
+    fft<false, PA, WarpSync>(v, t, X, lay, PassTable<PA, double>{});
     cpx<double> xa[EA / 2], xb[EA / 2];
-    split_pair<PA>(v, t, X, lay, xa, xb);
+    split_rows<PA, double>(v, t, X, RowLayout<N>{0}, xa, xb);
 #pragma unroll
     for (int m = 0; m < EA / 2; ++m) {
       S[(size_t)(2 * pr) * H + t + TA * m] = xa[m];
@@ -182,12 +168,12 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
     // ---- row A: c, bulk terms, history partials, F = x-FFT(f') into G.a ----
     {
       const int t = threadIdx.x % TA, pr = threadIdx.x / TA;
-      const RowLayout<N> lay{pr * RowLayout<N>::stride};
+      const SwizzleLayout<N, sizeof(cpx<double>)> lay{pr * N, (int)((threadIdx.x & 31) / TA)};
       const int la = 2 * pr, ya = y0 + la;
       cpx<double> v[EA];
 #pragma unroll
       for (int m = 0; m < EA; ++m) v[m] = pair_spectrum_sm<N>(S + (size_t)la * H, S + (size_t)(la + 1) * H, t + TA * m);
-      fft<true, PA>(v, t, X, lay, PassTable<PA, double>{});
+      fft<true, PA, WarpSync>(v, t, X, lay, PassTable<PA, double>{});
       double sc = 0.0, sf = 0.0, mn = INFINITY, mx = -INFINITY, bad = 0.0;
 #pragma unroll
       for (int m = 0; m < EA; ++m) {
@@ -203,54 +189,68 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
         bad += (double)((int)nonfinite_bits(ca) + (int)nonfinite_bits(cb));
         v[m] = mkc<double>(fa, fb);
       }
-      fft<false, PA>(v, t, X, lay, PassTable<PA, double>{});
+      __syncwarp();
+      fft<false, PA, WarpSync>(v, t, X, lay, PassTable<PA, double>{});
       cpx<double> xa[EA / 2], xb[EA / 2];
-      split_pair<PA>(v, t, X, lay, xa, xb);
+      split_rows<PA, double>(v, t, X, RowLayout<N>{0}, xa, xb);
 #pragma unroll
       for (int m = 0; m < EA / 2; ++m) {
         Gs[(size_t)la * H + t + TA * m].a = xa[m];
         Gs[(size_t)(la + 1) * H + t + TA * m].a = xb[m];
       }
-      double sums[3] = {sc, sf, bad};
-      block_sums<NW, 3>(sums, red);
-      const double bmn = block_minmax<NW>(mn, red + 3 * NW, false);
-      const double bmx = block_minmax<NW>(mx, red + 4 * NW, true);
-      if (threadIdx.x == 0) {
-        part[0] = sums[0];
-        part[1] = bmn;
-        part[2] = bmx;
-        part[3] = sums[1];
-        part[4] = sums[2];
+      // per-warp partials; the fold after the cluster barrier combines them
+      sc = warp_sum(sc);
+      sf = warp_sum(sf);
+      bad = warp_sum(bad);
+      mn = warp_min(mn);
+      mx = warp_max(mx);
+      if ((threadIdx.x & 31) == 0) {
+        const int wid = threadIdx.x >> 5;
+        part[0 * NW + wid] = sc;
+        part[1 * NW + wid] = mn;
+        part[2 * NW + wid] = mx;
+        part[3 * NW + wid] = sf;
+        part[4 * NW + wid] = bad;
       }
     }
     cl.sync();
     // fold row A's partials in rank order (every CTA the same totals)
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+      // lane l folds slots l, l + 32, ... of the C * NW (rank, warp) partials, then a
+      // fixed shuffle tree: the same order, hence the same bits, in every CTA
       double tsum = 0.0, tmin = INFINITY, tmax = -INFINITY, tf = 0.0, tbad = 0.0;
-      for (int r = 0; r < C; ++r) {
-        const double* q = cl.map_shared_rank(part, r);
-        tsum += q[0];
-        tmin = fmin(tmin, q[1]);
-        tmax = fmax(tmax, q[2]);
-        tf += q[3];
-        tbad += q[4];
+      for (int i = threadIdx.x; i < C * NW; i += 32) {
+        const double* q = cl.map_shared_rank(part, i / NW);
+        const int wq = i % NW;
+        tsum += q[0 * NW + wq];
+        tmin = fmin(tmin, q[1 * NW + wq]);
+        tmax = fmax(tmax, q[2 * NW + wq]);
+        tf += q[3 * NW + wq];
+        tbad += q[4 * NW + wq];
       }
-      fold[0] = tsum;
-      fold[1] = tmin;
-      fold[2] = tmax;
-      fold[3] = tf;
-      fold[4] = tbad;
-      if (rank == 0) {
-        const size_t ld = (size_t)a.hist_ld;
-        if (a.hist) {
-          a.hist[s] = (double)s * a.dt;
-          a.hist[s + ld] = tsum / NN;
-          a.hist[s + 3 * ld] = tmin;
-          a.hist[s + 4 * ld] = tmax;
-        }
-        if (tbad > 0.0) {
-          *a.bad_step = s;
-          *a.status = kStatusNonFinite;
+      tsum = warp_sum(tsum);
+      tf = warp_sum(tf);
+      tbad = warp_sum(tbad);
+      tmin = warp_min(tmin);
+      tmax = warp_max(tmax);
+      if (threadIdx.x == 0) {
+        fold[0] = tsum;
+        fold[1] = tmin;
+        fold[2] = tmax;
+        fold[3] = tf;
+        fold[4] = tbad;
+        if (rank == 0) {
+          const size_t ld = (size_t)a.hist_ld;
+          if (a.hist) {
+            a.hist[s] = (double)s * a.dt;
+            a.hist[s + ld] = tsum / NN;
+            a.hist[s + 3 * ld] = tmin;
+            a.hist[s + 4 * ld] = tmax;
+          }
+          if (tbad > 0.0) {
+            *a.bad_step = s;
+            *a.status = kStatusNonFinite;
+          }
         }
       }
     }
@@ -340,20 +340,20 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
         o.b = gy[m];
         dst[(size_t)(y % R) * H + kx] = o;
       }
-      double e1[1] = {gsum};
-      block_sums<NW, 1>(e1, red);
-      if (threadIdx.x == 0) part[5] = e1[0];
+      gsum = warp_sum(gsum);
+      if ((threadIdx.x & 31) == 0) part[5 * NW + (threadIdx.x >> 5)] = gsum;
     }
     cl.sync();
-    if (threadIdx.x == 0 && rank == 0) {
+    if (threadIdx.x < 32 && rank == 0) {
       double gr = 0.0;
-      for (int r = 0; r < C; ++r) gr += cl.map_shared_rank(part, r)[5];
-      if (a.hist) a.hist[s + 2 * (size_t)a.hist_ld] = (fold[3] + mp.kappa * gr / NN) * a.dx * a.dx;
+      for (int i = threadIdx.x; i < C * NW; i += 32) gr += cl.map_shared_rank(part, i / NW)[5 * NW + i % NW];
+      gr = warp_sum(gr);
+      if (threadIdx.x == 0 && a.hist) a.hist[s + 2 * (size_t)a.hist_ld] = (fold[3] + mp.kappa * gr / NN) * a.dx * a.dx;
     }
     // ---- row B: grad mu of own rows, M = M0 h(phi), dissipation, M grad mu -> G ----
     {
       const int t = threadIdx.x % TB, ry = threadIdx.x / TB;
-      const RowLayout<N> lay{ry * RowLayout<N>::stride};
+      const SwizzleLayout<N, sizeof(cpx<double>)> lay{ry * N, (int)((threadIdx.x & 31) / TB)};
       const int y = y0 + ry;
       cpx2<double>* row = Gs + (size_t)ry * H;
       cpx<double> v[EB];
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
         else
           v[m] = mkc<double>(va.x + vb.y, vb.x - va.y);
       }
-      fft<true, PB>(v, t, X, lay, PassTable<PB, double>{});
+      fft<true, PB, WarpSync>(v, t, X, lay, PassTable<PB, double>{});
       double dsum = 0.0;
 #pragma unroll
       for (int m = 0; m < EB; ++m) {
@@ -380,9 +380,10 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
         dsum += M * (v[m].x * v[m].x + v[m].y * v[m].y);
         v[m] = cscale(v[m], M);
       }
-      fft<false, PB>(v, t, X, lay, PassTable<PB, double>{});
+      __syncwarp();
+      fft<false, PB, WarpSync>(v, t, X, lay, PassTable<PB, double>{});
       cpx<double> xa[EB / 2], xb[EB / 2];
-      split_pair<PB>(v, t, X, lay, xa, xb);
+      split_rows<PB, double>(v, t, X, RowLayout<N>{0}, xa, xb);
 #pragma unroll
       for (int m = 0; m < EB / 2; ++m) {
         cpx2<double> o;
@@ -390,15 +391,15 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
         o.b = xb[m];
         row[t + TB * m] = o;
       }
-      double d1[1] = {dsum};
-      block_sums<NW, 1>(d1, red);
-      if (threadIdx.x == 0) part[6] = d1[0];
+      dsum = warp_sum(dsum);
+      if ((threadIdx.x & 31) == 0) part[6 * NW + (threadIdx.x >> 5)] = dsum;
     }
     cl.sync();
-    if (threadIdx.x == 0 && rank == 0) {
+    if (threadIdx.x < 32 && rank == 0) {
       double d = 0.0;
-      for (int r = 0; r < C; ++r) d += cl.map_shared_rank(part, r)[6];
-      if (a.hist) a.hist[s + 5 * (size_t)a.hist_ld] = d * a.dx * a.dx;
+      for (int i = threadIdx.x; i < C * NW; i += 32) d += cl.map_shared_rank(part, i / NW)[6 * NW + i % NW];
+      d = warp_sum(d);
+      if (threadIdx.x == 0 && a.hist) a.hist[s + 5 * (size_t)a.hist_ld] = d * a.dx * a.dx;
     }
     if (s == a.steps) break;  // the last history row: no update
 
@@ -485,12 +486,12 @@ __global__ void __launch_bounds__(Config<N>::TH, 1) k_cluster_run(const Args a) 
   // ---- S -> c (own row pairs), unless the run stopped on a non-finite field ----
   if (!stopped) {
     const int t = threadIdx.x % TA, pr = threadIdx.x / TA;
-    const RowLayout<N> lay{pr * RowLayout<N>::stride};
+    const SwizzleLayout<N, sizeof(cpx<double>)> lay{pr * N, (int)((threadIdx.x & 31) / TA)};
     const int la = 2 * pr, ya = y0 + la;
     cpx<double> v[EA];
 #pragma unroll
     for (int m = 0; m < EA; ++m) v[m] = pair_spectrum_sm<N>(S + (size_t)la * H, S + (size_t)(la + 1) * H, t + TA * m);
-    fft<true, PA>(v, t, X, lay, PassTable<PA, double>{});
+    fft<true, PA, WarpSync>(v, t, X, lay, PassTable<PA, double>{});
 #pragma unroll
     for (int m = 0; m < EA; ++m) {
       const int x = t + TA * m;
