@@ -4,8 +4,8 @@
 //
 // A single 256^2 or 128^2 particle gives each phase kernel of the launch-per-phase
 // path only a few warps per SM, so its steps cost the latency of four dependent
-// launches (about 10 us each) rather than their work.  Here C CTAs (16 for
-// n = 256, 8 for n = 128) share the grid: CTA r owns rows y in [r R, r R + R),
+// launches (about 10 us each) rather than their work.  Here C = 16 CTAs share
+// the grid: CTA r owns rows y in [r R, r R + R),
 // R = n / C, of the state S and of the pair array G (the f' transform F lives in
 // the first half of G's slots, which column A reads before it writes them).  The
 // four phases of a step are separated by hardware cluster barriers:
@@ -50,8 +50,8 @@ struct Config<256> {  // 16 CTAs of 256 threads: row pairs and columns 32 thread
   using B = CPlan<Plan<256, 16, Radices<16, 16>>>;
 };
 template <>
-struct Config<128> {  // 8 CTAs of 256 threads: row pairs and columns 32 x 4, rows 16 x 8
-  static constexpr int C = 8, TH = 256;
+struct Config<128> {  // 16 CTAs of 128 threads: row pairs and columns 32 x 4, rows 16 x 8
+  static constexpr int C = 16, TH = 128;
   using A = CPlan<Plan<128, 4, Radices<4, 4, 4, 2>>>;
   using B = CPlan<Plan<128, 8, Radices<8, 8, 2>>>;
 };

@@ -108,9 +108,10 @@ esc_status esc_wait(esc_ctx *ctx, int64_t *bad_step);
 esc_status esc_set_stream(esc_ctx *ctx, void *stream);
 
 /* 1 when runs of ctx go through the cluster-resident kernel: a single FP64 grid of n = 128
- * or 256 whose whole time loop runs in one launch of one thread-block cluster (16 CTAs for
- * 256, 8 for 128) with the state in distributed shared memory, when the device can place
- * the cluster and ESC_CLUSTER is not 0; else 0 (four launches per step). */
+ * or 256 whose whole time loop runs in one launch of one thread-block cluster of 16 CTAs
+ * with the state in distributed shared memory.  Chosen at creation when the device can place
+ * the cluster and 16 timed steps ran faster than the four-launch path (ESC_CLUSTER=1 forces
+ * it, 0 forbids it); else 0. */
 int esc_uses_cluster(const esc_ctx *ctx);
 
 /* Message of the last failure on ctx (ctx may be NULL: last failure of this thread). */
