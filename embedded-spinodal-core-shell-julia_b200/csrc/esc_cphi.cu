@@ -22,12 +22,13 @@ void esc_set_thread_error(const char* msg);
 namespace esc {
 namespace cphi {
 
-constexpr int kFdW = 16;  // adjacent z lines per block of the stencil kernels
+constexpr int kFdW = 16;     // adjacent z lines per block of the stencil kernels
+constexpr int kFdLoads = 8;  // staging sweeps whose loads are in flight together
 
 // div += D_a(M D_a mu) along axis a = x (0) or y (1): each block stages kFdW
 // adjacent z lines (n points each) of mu, of M = mobility h(phi) and of the
-// current div in shared memory -- every global load of the block is issued in
-// the first sweep --, turns the M tile into q = M D mu in place, then writes
+// current div in shared memory (the loads of kFdLoads sweeps in flight
+// together), turns the M tile into q = M D mu in place, then writes
 // div + D q.  Runtime n; dynamic shared memory 3 n kFdW doubles.
 __global__ void __launch_bounds__(kBlock) k3_fd_line(const Dev* __restrict__ dp, int axis) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -55,25 +56,58 @@ __global__ void __launch_bounds__(kBlock) k3_fd_line(const Dev* __restrict__ dp,
     r -= (r >= n) ? n : 0;
     return r * kFdW;
   };
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int p = idx / kFdW, w = idx % kFdW;
-    const bool ok = k0 + w < d.nz;
-    const long a = base + (long)p * estride + w;
-    mt[idx] = ok ? mu[a] : 0.0;
-    qt[idx] = ok ? mobility3(phi[a], M0) : 0.0;
-    dt[idx] = ok ? div[a] : 0.0;
+  // kFdLoads sweeps' loads are issued before any of them is stored: 3 kFdLoads
+  // loads in flight per thread instead of 3
+  for (int i0 = threadIdx.x; i0 < total; i0 += kFdLoads * blockDim.x) {
+    double lm[kFdLoads], lp[kFdLoads], ld[kFdLoads];
+#pragma unroll
+    for (int u = 0; u < kFdLoads; ++u) {
+      const int idx = i0 + u * (int)blockDim.x;
+      const int p = idx / kFdW, w = idx % kFdW;
+      const bool ok = idx < total && k0 + w < d.nz;
+      const long a = base + (long)p * estride + w;
+      lm[u] = ok ? mu[a] : 0.0;
+      lp[u] = ok ? phi[a] : 0.0;
+      ld[u] = ok ? div[a] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kFdLoads; ++u) {
+      const int idx = i0 + u * (int)blockDim.x;
+      if (idx >= total) break;
+      const bool ok = k0 + idx % kFdW < d.nz;
+      mt[idx] = lm[u];
+      qt[idx] = ok ? mobility3(lp[u], M0) : 0.0;
+      dt[idx] = ld[u];
+    }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int p = idx / kFdW, w = idx % kFdW;
-    qt[idx] *= fd4(mt[row(p, 2) + w], mt[row(p, 1) + w], mt[row(p, -1) + w], mt[row(p, -2) + w], inv12);
+  // thread (w, seg) sweeps rows [r0, r1) of line w with a five-point window in
+  // registers: one shared-memory load per point and stencil
+  const int w = threadIdx.x % kFdW, nseg = blockDim.x / kFdW;
+  const int rows = (n + nseg - 1) / nseg;
+  const int r0 = (threadIdx.x / kFdW) * rows, r1 = min(n, r0 + rows);
+  if (r0 < r1) {
+    double m2 = mt[row(r0, -2) + w], m1 = mt[row(r0, -1) + w], m0 = mt[r0 * kFdW + w], p1 = mt[row(r0, 1) + w];
+    for (int p = r0; p < r1; ++p) {
+      const double p2 = mt[row(p, 2) + w];
+      qt[p * kFdW + w] *= fd4(p2, p1, m1, m2, inv12);
+      m2 = m1;
+      m1 = m0;
+      m0 = p1;
+      p1 = p2;
+    }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int p = idx / kFdW, w = idx % kFdW;
-    if (k0 + w >= d.nz) continue;
-    div[base + (long)p * estride + w] =
-        dt[idx] + fd4(qt[row(p, 2) + w], qt[row(p, 1) + w], qt[row(p, -1) + w], qt[row(p, -2) + w], inv12);
+  if (r0 < r1 && k0 + w < d.nz) {
+    double m2 = qt[row(r0, -2) + w], m1 = qt[row(r0, -1) + w], m0 = qt[r0 * kFdW + w], p1 = qt[row(r0, 1) + w];
+    for (int p = r0; p < r1; ++p) {
+      const double p2 = qt[row(p, 2) + w];
+      div[base + (long)p * estride + w] = dt[p * kFdW + w] + fd4(p2, p1, m1, m2, inv12);
+      m2 = m1;
+      m1 = m0;
+      m0 = p1;
+      p1 = p2;
+    }
   }
 }
 

@@ -133,16 +133,22 @@ struct ZGeom {
   }
 };
 
-// forward z transforms.  kZInit: (c + i phi) of line q -> D1 = c^, D2 = phi^;
-// kZLocal: (df/dc + i df/dphi) of line q -> D1, D2; kZDiv: div of lines 2q, 2q+1 -> D1.
 // resident 256-thread blocks per SM the coupled kernels are compiled for
 template <class P>
 constexpr int cphi_minb() {
   return P::E <= 8 ? 2 : 1;
 }
-
+// the kernels that hold one transform's values at a time (z forward, strided
+// lines, final z inverse) fit 80 registers without spills at E <= 8: three blocks
 template <class P>
-__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zf(const Dev* __restrict__ dp, int mode) {
+constexpr int cphi_minb_light() {
+  return P::E <= 8 ? 3 : 1;
+}
+
+// forward z transforms.  kZInit: (c + i phi) of line q -> D1 = c^, D2 = phi^;
+// kZLocal: (df/dc + i df/dphi) of line q -> D1, D2; kZDiv: div of lines 2q, 2q+1 -> D1.
+template <class P>
+__global__ void __launch_bounds__(kBlock, cphi_minb_light<P>()) k3_zf(const Dev* __restrict__ dp, int mode) {
   using ZG = ZGeom<P>;
   constexpr int N = ZG::N, E = ZG::E, T = ZG::T, G = ZG::G, K = ZG::K;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -326,7 +332,7 @@ __device__ __forceinline__ bool six_fold(const Six& mine, double* part, unsigned
 
 // inverse z transform of (c^' + i phi^') per line -> c, phi; history row and stop checks
 template <class P>
-__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_final(const Dev* __restrict__ dp, int s_local) {
+__global__ void __launch_bounds__(kBlock, cphi_minb_light<P>()) k3_zi_final(const Dev* __restrict__ dp, int s_local) {
   using ZG = ZGeom<P>;
   constexpr int N = ZG::N, E = ZG::E, T = ZG::T, G = ZG::G, K = ZG::K;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -410,7 +416,7 @@ struct LGeom {
 // in-place transforms of na (1 or 2) arrays along a strided axis: element p of
 // line (o, kz) at o*ostride + kz + p*estride
 template <class P, bool INV>
-__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_line(const Dev* __restrict__ dp, double2* a0, double2* a1, int na,
+__global__ void __launch_bounds__(kBlock, cphi_minb_light<P>()) k3_line(const Dev* __restrict__ dp, double2* a0, double2* a1, int na,
                                                   long estride, long ostride) {
   using LG = LGeom<P>;
   constexpr int E = LG::E, T = LG::T, W = LG::W;
