@@ -220,6 +220,12 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_mu(const Dev* __
   for (int m = 0; m < E; ++m)
     v[m] = active ? merge_half<N>(d.D1 + la * K, hasb ? d.D1 + (la + 1) * K : nullptr, t + T * m)
                   : mkc<double>(0.0, 0.0);
+  if (active) {
+    // phi is read after the transform: pull the pair's lines into L2 now (one
+    // prefetch per 128-byte line, 16 doubles)
+    const int count = (hasb ? 2 : 1) * N;
+    for (int i = 16 * t; i < count; i += 16 * T) prefetch_l2(d.phi + la * N + i);
+  }
   cpx<double>* sm = reinterpret_cast<cpx<double>*>(smraw);
   const auto lay = ZG::layout(g);
   fft<true, P, typename ZG::Sync>(v, t, sm, lay, PassTable<P, double>{});
@@ -506,7 +512,7 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
     // mu^ = FFT(df/dc) + 2 kappa_c k^2 c^ (Compute_mu), back along x
     load(d.D1, v);
     prefetch(d.Ch);
-    prefetch(d.Ph);
+    prefetch(d.D2);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     const double kc2 = 2.0 * d.p.kappa_c;
 #pragma unroll
@@ -520,6 +526,7 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
     store(d.D1, v);
     // phi^' = (phi^ - L dt FFT(df/dphi)) / (1 + 2 L kappa_phi k^2 dt)
     load(d.D2, v);
+    prefetch(d.Ph);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     const double Ldt = d.p.relax * d.dt, c2 = 2.0 * d.p.relax * d.p.kappa_phi * d.dt;
 #pragma unroll
@@ -534,6 +541,7 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
     // c^' = (dt div^ + lhs c^) / lhs, lhs = 1 + 2 Q kappa_c k^4 dt (kernel_comp_phi)
     load(d.D1, v);
     prefetch(d.Ch);
+    prefetch(d.Ph);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     const double c1 = 2.0 * d.p.Q * d.p.kappa_c * d.dt;
 #pragma unroll
