@@ -451,11 +451,15 @@ __global__ void __launch_bounds__(kBlock, cphi_minb_light<P>()) k3_line(const De
   }
 }
 
-// x pass with the spectral operations (lines (j, kz), element kx; o = j = blockIdx.y)
+// x pass with the spectral operations (lines (j, kz), element kx; o = j = blockIdx.y).
+// A step's two x passes (kXMu, kXUpdate) each launch two kernels, one per chain of
+// transforms (composition, order parameter): a kernel holds one line's values at a
+// time, which fits three blocks per SM (two for the mu chain, which would spill).
 enum XOp { kXInit = 0, kXMu = 1, kXUpdate = 2 };
+enum XKernel { kXKInit = 0, kXKMu = 1, kXKPhi = 2, kXKUpdC = 3, kXKPhiInv = 4 };
 
 template <class P, int OP>
-__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __restrict__ dp, int s_local) {
+__global__ void __launch_bounds__(kBlock, OP == kXKMu ? cphi_minb<P>() : cphi_minb_light<P>()) k3_xspec(const Dev* __restrict__ dp, int s_local) {
   using LG = LGeom<P>;
   constexpr int N = LG::N, E = LG::E, T = LG::T, W = LG::W;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -501,18 +505,17 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
     }
   };
   cpx<double> v[E];
-  if (OP == kXInit) {
+  if (OP == kXKInit) {
     load(d.D1, v);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     store(d.Ch, v);
     load(d.D2, v);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     store(d.Ph, v);
-  } else if (OP == kXMu) {
+  } else if (OP == kXKMu) {
     // mu^ = FFT(df/dc) + 2 kappa_c k^2 c^ (Compute_mu), back along x
     load(d.D1, v);
     prefetch(d.Ch);
-    prefetch(d.D2);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     const double kc2 = 2.0 * d.p.kappa_c;
 #pragma unroll
@@ -524,6 +527,7 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
     }
     fft<true, P>(v, t, sm, lay, PassTable<P, double>{});
     store(d.D1, v);
+  } else if (OP == kXKPhi) {
     // phi^' = (phi^ - L dt FFT(df/dphi)) / (1 + 2 L kappa_phi k^2 dt)
     load(d.D2, v);
     prefetch(d.Ph);
@@ -537,11 +541,10 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
       v[m] = mkc<double>((ph.x - Ldt * v[m].x) / lhse, (ph.y - Ldt * v[m].y) / lhse);
     }
     store(d.Ph, v);
-  } else {
+  } else if (OP == kXKUpdC) {
     // c^' = (dt div^ + lhs c^) / lhs, lhs = 1 + 2 Q kappa_c k^4 dt (kernel_comp_phi)
     load(d.D1, v);
     prefetch(d.Ch);
-    prefetch(d.Ph);
     fft<false, P>(v, t, sm, lay, PassTable<P, double>{});
     const double c1 = 2.0 * d.p.Q * d.p.kappa_c * d.dt;
 #pragma unroll
@@ -563,6 +566,8 @@ __global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_xspec(const Dev* __
     store(d.Ch, v);
     fft<true, P>(v, t, sm, lay, PassTable<P, double>{});
     store(d.D1, v);
+  } else {
+    // phi^' back along x
     load(d.Ph, v);
     fft<true, P>(v, t, sm, lay, PassTable<P, double>{});
     store(d.D2, v);
@@ -624,9 +629,11 @@ struct SetOf {
     if ((e = cudaFuncSetAttribute(k3_zi_final<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs))) return e;
     if ((e = cudaFuncSetAttribute(k3_line<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
     if ((e = cudaFuncSetAttribute(k3_line<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
-    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXInit>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
-    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXMu>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
-    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls)))
+    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXKInit>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
+    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXKMu>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
+    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXKPhi>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
+    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXKUpdC>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
+    if ((e = cudaFuncSetAttribute(k3_xspec<P, kXKPhiInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls)))
       return e;
     return cudaSuccess;
   }
@@ -645,12 +652,15 @@ struct SetOf {
       k3_line<P, false><<<grid, kBlock, LG::smem(), st>>>(d, a0, a1, na, es, os);
   }
   static void xspec(const Dev* d, int op, int s_local, dim3 grid, cudaStream_t st) {
-    if (op == kXInit)
-      k3_xspec<P, kXInit><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
-    else if (op == kXMu)
-      k3_xspec<P, kXMu><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
-    else
-      k3_xspec<P, kXUpdate><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
+    if (op == kXInit) {
+      k3_xspec<P, kXKInit><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
+    } else if (op == kXMu) {
+      k3_xspec<P, kXKMu><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
+      k3_xspec<P, kXKPhi><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
+    } else {
+      k3_xspec<P, kXKUpdC><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
+      k3_xspec<P, kXKPhiInv><<<grid, kBlock, LG::smem(), st>>>(d, s_local);
+    }
   }
   static Set make() {
     Set s;
