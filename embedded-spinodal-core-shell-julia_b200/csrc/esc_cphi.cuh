@@ -144,11 +144,16 @@ template <class P>
 constexpr int cphi_minb_light() {
   return P::E <= 8 ? 3 : 1;
 }
+// the z forward kernel fits 64 registers without spills at E <= 8: four blocks
+template <class P>
+constexpr int cphi_minb_zf() {
+  return P::E <= 8 ? 4 : 1;
+}
 
 // forward z transforms.  kZInit: (c + i phi) of line q -> D1 = c^, D2 = phi^;
 // kZLocal: (df/dc + i df/dphi) of line q -> D1, D2; kZDiv: div of lines 2q, 2q+1 -> D1.
 template <class P>
-__global__ void __launch_bounds__(kBlock, cphi_minb_light<P>()) k3_zf(const Dev* __restrict__ dp, int mode) {
+__global__ void __launch_bounds__(kBlock, cphi_minb_zf<P>()) k3_zf(const Dev* __restrict__ dp, int mode) {
   using ZG = ZGeom<P>;
   constexpr int N = ZG::N, E = ZG::E, T = ZG::T, G = ZG::G, K = ZG::K;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -203,7 +208,7 @@ __global__ void __launch_bounds__(kBlock, cphi_minb_light<P>()) k3_zf(const Dev*
 // inverse z transform of mu^ (lines 2q, 2q+1 of D1 in one complex FFT), then the
 // z part of div: D_z(M D_z mu) along the line; writes mu and div
 template <class P>
-__global__ void __launch_bounds__(kBlock, cphi_minb<P>()) k3_zi_mu(const Dev* __restrict__ dp) {
+__global__ void __launch_bounds__(kBlock, cphi_minb_light<P>()) k3_zi_mu(const Dev* __restrict__ dp) {
   using ZG = ZGeom<P>;
   constexpr int N = ZG::N, E = ZG::E, T = ZG::T, G = ZG::G, K = ZG::K;
   extern __shared__ __align__(16) unsigned char smraw[];
