@@ -306,7 +306,7 @@ def large_grid_configs(peak_gbs):
 
 
 def coupled_kernel_bytes(nx, ny, nz):
-    """Bytes each of the twelve kernels of a coupled step must move (FP64: real fields 8 B
+    """Bytes each of the twelve stages of a coupled step must move (FP64: real fields 8 B
     per point, half spectra 16 B per mode, nx*ny*(nz/2+1) modes), in launch order."""
     n3 = nx * ny * nz
     nk = nx * ny * (nz // 2 + 1)

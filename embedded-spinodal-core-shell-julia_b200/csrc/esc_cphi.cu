@@ -264,9 +264,9 @@ std::mutex& cphi_mutex() {
   return m;
 }
 
-// One step of the coupled model (twelve launches), s_local its index inside the
-// chunk.  With `ev` (13 events), ev[k] is recorded before launch k and ev[12]
-// after the last (per-kernel timing).
+// One step of the coupled model (twelve stages, fourteen launches), s_local its
+// index inside the chunk.  With `ev` (13 events), ev[k] is recorded before stage
+// k and ev[12] after the last (per-stage timing).
 constexpr int kStepKernels = 12;
 void launch_step(esc_cphi& X, int s_local, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   using namespace esc::cphi;

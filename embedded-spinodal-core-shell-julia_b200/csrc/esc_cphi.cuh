@@ -17,11 +17,12 @@
 // kept real (the Re IFFT projection).  A 3-D transform is a z pass (two real
 // lines packed into one complex FFT and split), a y pass and an x pass over
 // strided lines (W adjacent kz lines per block, so every row of a tile is a
-// contiguous segment).  Per step, twelve launches:
+// contiguous segment).  Per step, twelve stages (the x passes launch one kernel per
+// chain of transforms, so fourteen launches):
 //   zf(local)  c, phi lines -> df/dc + i df/dphi -> z-FFT -> D1, D2 half spectra
 //   y fwd      D1, D2
 //   x spec 1   x-FFT D1 -> mu^ = D1 + 2 kappa_c k^2 C^ -> inverse x-FFT -> D1;
-//              x-FFT D2 -> Ph = (Ph - L dt D2)/(1 + 2 L kappa_phi k^2 dt)
+//              then x-FFT D2 -> Ph = (Ph - L dt D2)/(1 + 2 L kappa_phi k^2 dt)
 //   y inv      D1
 //   zi(mu)     D1 -> mu (two lines per complex inverse FFT) -> mu; fourth-order
 //              z derivative, M, again -> div (the z part)
@@ -29,7 +30,7 @@
 //   zf(div)    div lines in pairs -> z-FFT -> D1
 //   y fwd      D1
 //   x spec 2   x-FFT D1 -> C^ = (dt div^ + lhs C^)/lhs (mass check at k = 0) ->
-//              inverse x-FFT -> D1;  Ph -> inverse x-FFT -> D2
+//              inverse x-FFT -> D1;  then Ph -> inverse x-FFT -> D2
 //   y inv      D1, D2
 //   zi(final)  c + i phi from D1, D2 -> c, phi; history row, bounds,
 //              convergence and non-finite checks (last-arriver fold)

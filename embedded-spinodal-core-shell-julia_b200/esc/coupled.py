@@ -117,7 +117,7 @@ class Coupled:
                "x stencil", "z fwd div", "y fwd", "x c update", "y inv x2", "z inv final")
 
     def profile(self, steps: int = 5):
-        """Mean time (ms) of each of the twelve kernels of a step (esc_cphi_profile),
+        """Mean time (ms) of each of the twelve stages of a step (esc_cphi_profile),
         stepping on from the fields of the last run."""
         ms = np.zeros(12)
         st = load_library().esc_cphi_profile(self._h, int(steps), _ptr(ms))

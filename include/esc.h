@@ -313,8 +313,9 @@ esc_status esc_cphi_run_device(esc_cphi *ctx, double *c, double *phi, int steps,
 esc_status esc_cphi_set_stream(esc_cphi *ctx, void *stream);
 
 /* Measurement aid: steps on from the fields the last run left, `steps` times, timing
- * each of the twelve kernels of a step with CUDA events on the context's stream;
- * ms[k] (12 values) gets the mean time of kernel k in launch order: z forward of the
+ * each of the twelve stages of a step with CUDA events on the context's stream (the two
+ * x passes are two kernels each, timed together); ms[k] (12 values) gets the mean time
+ * of stage k in launch order: z forward of the
  * local terms, y forward (2 fields), x pass with mu^ and the phi update, y inverse,
  * z inverse of mu with the z stencil, y stencil, x stencil, z forward of div,
  * y forward, x pass with the c update, y inverse (2 fields), z inverse to c and phi. */
