@@ -44,6 +44,9 @@ def run_both(shape, spacing, steps, p=co.CoupledParameters(), seed=1, radius=Non
     ((32, 24, 48), (1.0, 1.0, 1.0), 20),
     ((8, 12, 64), (0.8, 1.0, 1.2), 15),
     ((64, 64, 64), (1.0, 1.0, 1.0), 10),
+    # the eight-element 128- and 256-point plans on every axis (the plans of the 256^3 bench)
+    ((8, 128, 256), (1.0, 1.0, 1.0), 6),
+    ((256, 16, 128), (1.0, 1.1, 0.9), 6),
 ])
 def test_coupled_matches_oracle(shape, spacing, steps):
     (c, phi, h, done, reason), (co_, pho, ho, doneo, reasono) = run_both(shape, spacing, steps)
