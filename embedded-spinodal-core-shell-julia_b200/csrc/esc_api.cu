@@ -917,9 +917,10 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
   TRY(ensure_graph(E));
   // Every group runs on its own stream, forked from (and joined back into) the
   // caller's stream: H2D of its fields, the steps, the final history row, and
-  // (below) its D2H copies.  The smallest groups are queued first, so that
-  // steps start while the larger fields are still being copied in; the
-  // largest group has the highest stream priority and finishes first.
+  // (below) its D2H copies.  The smallest group is queued first and the largest
+  // second, then the rest in ascending size, so that steps start while the other
+  // fields are still being copied in; the largest group has the highest stream
+  // priority and finishes first.
   const int ng = (int)E.groups.size();
   std::vector<int> order(ng);
   for (int gi = 0; gi < ng; ++gi) order[gi] = gi;
@@ -927,6 +928,9 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
     const Group &ga = E.groups[a], &gb = E.groups[b];
     return (double)ga.members.size() * ga.n * ga.n < (double)gb.members.size() * gb.n * gb.n;
   });
+  // then the largest group second: it carries the most steps' work, so its fields
+  // come in right after the first (smallest) group has started the GPU
+  if (ng > 2) std::rotate(order.begin() + 1, order.end() - 1, order.end());
   CK(cudaEventRecord(E.fork_ev, st));
   for (int gi : order) {
     Group& g = E.groups[gi];
