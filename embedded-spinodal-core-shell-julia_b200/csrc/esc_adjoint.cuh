@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col1_m(cons
 
 
 template <class P>
-__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col2_m(const AdjDev* __restrict__ adjs) {
+__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 3 : 1)) k_adj_col2_m(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, W = ColGeom<P>::W;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32 * 4];
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_col2_m(cons
 
 
 template <class P>
-__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 2 : 1)) k_adj_row2_m(const AdjDev* __restrict__ adjs) {
+__global__ void __launch_bounds__(kBlock, (P::E <= 8 ? 3 : 1)) k_adj_row2_m(const AdjDev* __restrict__ adjs) {
   constexpr int N = P::N, E = P::E, T = P::T, H = N / 2, G = RowGeom<P>::G;
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double red[32 * 4];
