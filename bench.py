@@ -41,6 +41,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -89,14 +90,65 @@ def read_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """SM clock, power and throttle-reason sampling during the timed region.
 
-    def __init__(self, index: int):
+    Reads NVML in a thread of this process (the counters `nvidia-smi --query-gpu` prints). A
+    separate nvidia-smi process was measured to stall the GPU's work now and then (one timed
+    region in four 9-45 % slow, SM clock at its maximum), the in-process sampler never did; the
+    nvidia-smi process remains the fallback when NVML cannot be loaded."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
+
+    def __init__(self, index: int, period_s: float = 0.1):
         self.index = index
+        self.period_s = period_s
         self.proc = None
         self.path = None
+        self.thread = None
+        self.samples = []
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _nvml_sample(self):
+        nv, h = self._nv, self._h
+        try:
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                             float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                             nv.nvmlDeviceGetPowerUsage(h) / 1000.0, int(reasons)))
+
+    def _nvml_loop(self):
+        while not self._stop.wait(self.period_s):
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
 
     def __enter__(self):
+        try:
+            self._nv, self._h = self._nvml_handle()
+            self._nvml_sample()
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            self.source = "nvml"
+            return self
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -107,12 +159,29 @@ class ClockSampler:
                  "clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # nvidia-smi's start-up (driver initialisation over every GPU of the node) can
+            # stall work on this GPU: wait for its first sample before anything is timed
+            t_end = time.time() + 10.0
+            while time.time() < t_end and self.proc.poll() is None:
+                with open(self.path) as f:
+                    if f.readline():
+                        break
+                time.sleep(0.02)
             time.sleep(0.3)
+            self.source = "nvidia-smi"
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join()
+            try:
+                self._nvml_sample()
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -120,32 +189,41 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def _read_smi(self):
         if not self.path or not os.path.exists(self.path):
-            return None
-        sm, mx, pw, reasons = [], [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            return
+        names = [nm for nm, _ in self.REASONS]
+        bits = dict(self.REASONS)
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 7:
                 continue
             try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
+                sm, mx = float(parts[0]), float(parts[1])
             except ValueError:
                 continue
             try:
-                pw.append(float(parts[2]))
+                pw = float(parts[2])
             except ValueError:
-                pass
+                pw = None
+            mask = 0
             for nm, v in zip(names, parts[3:7]):
                 if v.lower() == "active":
-                    reasons.add(nm)
+                    mask |= bits[nm]
+            self.samples.append((sm, mx, pw, mask))
         os.unlink(self.path)
-        if not sm:
+        self.path = None
+
+    def summary(self):
+        self._read_smi()
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "power_w": statistics.median(pw) if pw else None, "samples": len(sm)}
+        sm = [s[0] for s in self.samples]
+        pw = [s[2] for s in self.samples if s[2] is not None]
+        reasons = sorted(nm for nm, bit in self.REASONS if any(s[3] & bit for s in self.samples))
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": reasons, "power_w": statistics.median(pw) if pw else None,
+                "samples": len(sm), "source": self.source}
 
 
 def cpu_oracle_rate(ns, phis, c0s, ps, steps, workers):
