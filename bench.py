@@ -100,7 +100,7 @@ class ClockSampler:
     REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
                ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
-    def __init__(self, index: int, period_s: float = 0.1):
+    def __init__(self, index: int, period_s: float = 0.025):
         self.index = index
         self.period_s = period_s
         self.proc = None
