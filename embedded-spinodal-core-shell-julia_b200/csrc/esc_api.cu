@@ -172,6 +172,30 @@ int split_factor() {
   return k >= 1 && k <= 8 ? k : 1;
 }
 
+// ESC_H2D_ORDER = i0,i1,...: the queue order of the groups in a host-buffer batch
+// run, as indices into the groups sorted by ascending points (measurement aid;
+// an order that does not name every group once is ignored).
+bool h2d_order_knob(std::vector<int>& pos, int ng) {
+  const char* v = getenv("ESC_H2D_ORDER");
+  if (!v) return false;
+  pos.clear();
+  for (const char* q = v; *q;) {
+    char* e = nullptr;
+    const long k = strtol(q, &e, 10);
+    if (e == q || k < 0 || k >= ng) return false;
+    pos.push_back((int)k);
+    q = *e == ',' ? e + 1 : e;
+    if (*e && *e != ',') return false;
+  }
+  if ((int)pos.size() != ng) return false;
+  std::vector<char> seen(ng, 0);
+  for (int k : pos) {
+    if (seen[k]) return false;
+    seen[k] = 1;
+  }
+  return true;
+}
+
 // ESC_ROWS = warp | pipe | legacy forces one row-kernel family (measurement aid)
 int row_family_override() {
   const char* v = getenv("ESC_ROWS");
@@ -917,9 +941,9 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
   TRY(ensure_graph(E));
   // Every group runs on its own stream, forked from (and joined back into) the
   // caller's stream: H2D of its fields, the steps, the final history row, and
-  // (below) its D2H copies.  The smallest group is queued first and the largest
-  // second, then the rest in ascending size, so that steps start while the other
-  // fields are still being copied in; the largest group has the highest stream
+  // (below) its D2H copies.  The groups are queued in ascending size, so that steps
+  // start while the other fields are still being copied in, except that the largest
+  // group comes before the second largest; the largest group has the highest stream
   // priority and finishes first.
   const int ng = (int)E.groups.size();
   std::vector<int> order(ng);
@@ -928,9 +952,15 @@ esc_status engine_run(Engine& E, double* const* cptr, bool device_io, int steps,
     const Group &ga = E.groups[a], &gb = E.groups[b];
     return (double)ga.members.size() * ga.n * ga.n < (double)gb.members.size() * gb.n * gb.n;
   });
-  // then the largest group second: it carries the most steps' work, so its fields
-  // come in right after the first (smallest) group has started the GPU
-  if (ng > 2) std::rotate(order.begin() + 1, order.end() - 1, order.end());
+  // then the largest group before the second largest: with the highest priority it
+  // finishes before the second largest, whose last steps cover its D2H copies
+  std::vector<int> pos;
+  if (h2d_order_knob(pos, ng)) {
+    std::vector<int> asc = order;
+    for (int k = 0; k < ng; ++k) order[k] = asc[pos[k]];
+  } else if (ng > 2) {
+    std::swap(order[ng - 2], order[ng - 1]);
+  }
   CK(cudaEventRecord(E.fork_ev, st));
   for (int gi : order) {
     Group& g = E.groups[gi];
