@@ -614,6 +614,14 @@ esc_status autotune(Engine& E) {
   const bool timing = tuning_enabled() && row_family_override() < 0 && pipeline_enabled();
   bool any = false;
   for (Group& g : E.groups) {
+    // the runtime-size kernels have one family each: nothing to time, and their
+    // group must neither read nor write the decisions kept for a tuned set of the
+    // same (n, precision, count), whose column family 2 they do not have
+    if (g.ks->generic) {
+      apply_rows(g, 0);
+      apply_cols(g, 0);
+      continue;
+    }
     const bool can_pipe_rows = g.pipe_rows, can_warp = g.warp_rows, can_pipe_cols = g.pipe_cols;
     const TuneKey key{g.n, E.prec, (int)g.members.size()};
     auto hit = tune_cache().find(key);
@@ -622,8 +630,10 @@ esc_status autotune(Engine& E) {
     if (use_cache && hit != tune_cache().end()) {
       int r = hit->second.first, k = hit->second.second;
       if ((r == 2 && !can_warp) || (r == 1 && !can_pipe_rows)) r = 0;
+      // a decision read from a file may name a family this kernel set lacks
+      if ((k == 1 && !can_pipe_cols) || (k == 2 && g.ks->E_alt == g.ks->E) || k < 0 || k > 2) k = 0;
       apply_rows(g, r);
-      apply_cols(g, (k == 1 && !can_pipe_cols) ? 0 : k);
+      apply_cols(g, k);
       continue;
     }
     if (!timing) {

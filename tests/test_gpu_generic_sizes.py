@@ -102,3 +102,38 @@ def test_generic_nonfinite_reports_step_and_keeps_c():
     with pytest.raises(esc.NonFiniteError) as ei:
         esc.run_simulation(bad, phi, dt=0.01, steps=4)
     assert ei.value.step == 0
+
+
+_CACHED_CHILD = r"""
+import sys
+import numpy as np
+import esc
+from oracle import core_shell_oracle as orc
+n = int(sys.argv[1])
+c0, phi = orc.initial_fields(n, radius=0.3 * n, width=max(1.0, n / 64), seed=5)
+c, h = esc.run_simulation(c0, phi, dt=0.01, steps=9)
+np.savez(sys.argv[2], c=c, h=h, c0=c0, phi=phi)
+"""
+
+
+@pytest.mark.parametrize("n", [128, 256])
+def test_forced_generic_ignores_cached_tuned_decisions(n, tmp_path):
+    """A decision the tuner kept for the tuned kernel set of the same (n, precision,
+    instance count) -- here the alternative column plan with warp rows, as a tuner
+    cache file holds it -- does not apply to the runtime-size kernels, which have
+    one family each.  Fresh process: the cache file is read once per process."""
+    import subprocess
+    import sys
+    cache = tmp_path / "tune.jsonl"
+    cache.write_text("".join(f'{{"n": {n}, "prec": {p}, "count": 1, "rows": 2, "cols": 2}}\n' for p in (0, 1)))
+    out = tmp_path / "run.npz"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, ESC_TUNE_CACHE=str(cache), ESC_GENERIC="1",
+               PYTHONPATH=os.pathsep.join([root, os.path.join(root, "embedded-spinodal-core-shell-julia_b200"),
+                                           os.environ.get("PYTHONPATH", "")]))
+    r = subprocess.run([sys.executable, "-c", _CACHED_CHILD, str(n), str(out)], env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = np.load(out)
+    co, ho = oracle(d["c0"], d["phi"], 9)
+    assert rel(d["c"], co) < RTOL_FP64 and hist_rel(d["h"], ho) < RTOL_FP64
