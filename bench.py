@@ -255,11 +255,22 @@ def sample_subset(ns, k_per_size=1):
     return out
 
 
+def ensemble_config(count, sizes, pts, world):
+    """The `config` both arms print for the batched-ensemble workload."""
+    return {"workload": f"batched ensemble: {count} particles per GPU, n in {list(sizes)}, "
+                        f"{pts} points, dt=0.01, mixed precision",
+            "global_batch": count * world, "l2": "working set 1.7 GB >> 126 MB L2; no flush"}
+
+
 def run_reference(args, world, rank):
-    """CPU oracle on a bounded sample of the ensemble; rank 0 only."""
+    """CPU oracle on a bounded sample of the ensemble; rank 0 only.  The line carries the
+    ensemble's own config (the rate is per point-step, so a sample of the workload measures it);
+    `cpu_baseline.sample` names the sample."""
     if rank != 0:
         return 0
-    ns, phis, c0s, ps = ensemble(count=64)
+    sizes = [int(x) for x in args.sizes.split(",")]
+    ns, phis, c0s, ps = ensemble(count=args.count, seed_base=0, rng_seed=0, sizes=sizes)
+    full_pts = sum(n * n for n in ns)
     idx = sample_subset(ns)          # one particle of each grid size
     sub = [ns[i] for i in idx], [phis[i] for i in idx], [c0s[i] for i in idx], [ps[i] for i in idx]
     workers = os.cpu_count() or 1
@@ -273,10 +284,10 @@ def run_reference(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "batched ensemble sample: one particle of each size "
-                               f"{sorted(set(sub[0]))}, {pts} points, dt=0.01"},
+        "config": ensemble_config(args.count, sizes, full_pts, world),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": workers, "kind": "port",
-                         "sample": f"{len(idx)} particles ({pts} points) x {args.steps} steps; "
+                         "sample": f"{len(idx)} particles of the ensemble, one of each size "
+                                   f"{sorted(set(sub[0]))} ({pts} points) x {args.steps} steps; "
                                    "NumPy/scipy.fft restatement of core_shell.jl (Julia absent)"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -740,9 +751,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 state / f32 flux transforms",
         "data": "synthetic",
-        "config": {"workload": f"batched ensemble: {args.count} particles per GPU, n in {list(sizes)}, "
-                               f"{pts} points, dt=0.01, mixed precision",
-                   "global_batch": args.count * world, "l2": "working set 1.7 GB >> 126 MB L2; no flush"},
+        "config": ensemble_config(args.count, sizes, pts, world),
         "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
         "fp64_dropin": fp64, "max_abs_err_vs_fp64": max_err, "accuracy": accuracy, "large_grids": large,
         "clocks": clocks,

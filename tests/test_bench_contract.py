@@ -26,7 +26,12 @@ def test_reference_arm_json_line():
     assert line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
-    assert "workload" in line["config"]
+    # the GPU arm's own config (same workload, same point count), the sample named in cpu_baseline
+    sys.path.insert(0, ROOT)
+    import bench
+    ns = bench.ensemble()[0]
+    assert line["config"] == bench.ensemble_config(bench.COUNT, bench.SIZES, sum(n * n for n in ns), 1)
+    assert "one of each size" in line["cpu_baseline"]["sample"]
 
 
 def test_reference_arm_other_ranks_exit_quietly():
